@@ -1,0 +1,72 @@
+/*
+ * posit_gpu.h -- C ABI of the B200 posit32 BLAS (libposit_gpu_b200.so).
+ *
+ * A posit32 is passed as its raw 32-bit pattern (uint32_t): the SoftPosit posit32
+ * class of the reference is one 32-bit word (member `value`), so a posit32* is a
+ * uint32_t* and a posit32 argument is its `.value`.  Matrices are column-major with
+ * leading dimensions, exactly as in the reference.
+ *
+ * Return codes: 0 on success; 1..13 is the BLAS "info" of the first bad argument (the
+ * number the reference hands to Mxerbla, which exits -- here it is returned);
+ * negative values are POSIT_E_* below.
+ */
+#ifndef POSIT_GPU_H
+#define POSIT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define POSIT_E_CUDA (-1)         /* a CUDA runtime call failed (see posit_last_cuda_error) */
+#define POSIT_E_NO_DEVICE (-2)    /* no usable CUDA device */
+#define POSIT_E_NO_MEMORY (-3)    /* device or pinned-host allocation failed */
+#define POSIT_E_DEVICE_FAULT (-4) /* a kernel raised its error flag (bounded wait expired) */
+#define POSIT_E_WORKSPACE (-5)    /* caller-provided workspace too small */
+
+/* Replaces initOpenCL (libRpack/def.h:63, libRpack/Rgemm_opencl.cpp:59-70): selects
+ * the current CUDA device, creates its context and warms the kernels.  Optional: every
+ * entry point initialises lazily.  Returns 0 or a POSIT_E_* code. */
+int posit_init(void);
+
+/* C <- alpha*op(A)*op(B) + beta*C on HOST buffers, synchronous.
+ * Replaces RgemmG (libRpack/mpblas_posit.h:49-55, libRpack/Rgemm_opencl.cpp:199-250)
+ * and has the semantics of the CPU Rgemm (libRpack/Rgemm.cpp:62-251): transa/transb
+ * are 'N', 'T' or 'C' in either case ('C' means transposed; RgemmG treated it as 'N'),
+ * argument checks return the Rgemm info code, quick returns as in Rgemm.cpp:134-157,
+ * and per-element operation order as in Rgemm.cpp:163-247, so results are bit-identical
+ * to the CPU Rgemm for every transpose case.  Unlike RgemmG there is no CPU path for
+ * small m or n (Rgemm_opencl.cpp:232-235), and only the m x n submatrix of C is read
+ * and written (RgemmG copies whole ldc*n spans). */
+int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc);
+
+/* Device-memory form of posit_rgemm: A, B, C are device pointers; the call is
+ * asynchronous on `stream` (a cudaStream_t; NULL = the calling thread's default
+ * stream).  `workspace` may be NULL, in which case a stream-ordered allocation of
+ * posit_rgemm_workspace_size() bytes is made and freed on `stream`; otherwise it must be
+ * a device buffer of at least that many bytes, 16-byte aligned, not in use by another
+ * call in flight.  No reference counterpart: the reference ships host buffers on every
+ * call (Rgemm_opencl.cpp:165-173); this is what keeps factorizations device-resident. */
+int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                    int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
+                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* Bytes of device workspace posit_rgemm_dev needs for this shape (0 when none). */
+size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k);
+
+/* Reads (and with clear != 0 resets) the device-side error flags raised by kernels. */
+int posit_device_error(int clear);
+
+/* The last CUDA error code seen by the library (cudaError_t value). */
+int posit_last_cuda_error(void);
+
+/* Human-readable text for a return code. */
+const char *posit_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POSIT_GPU_H */

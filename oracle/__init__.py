@@ -1,0 +1,138 @@
+"""ctypes access to the oracle (test infrastructure only).
+
+``orc``  -- the CPU restatement in ``posit_oracle.c`` (``liborc.so``; built on demand
+            with gcc if missing).
+``ref``  -- the reference's own sources compiled here (``_ref/libposit_ref.so``), or
+            ``None`` where it was not built (it needs the reference tree).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+may use this package, and only as the checker / CPU baseline.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_U32P = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_c = ctypes
+
+
+def _load_orc():
+    path = os.path.join(HERE, "liborc.so")
+    if not os.path.exists(path):
+        from . import build_oracle
+        build_oracle.build_oracle()
+    lib = ctypes.CDLL(path)
+    u32, i32, i64 = _c.c_uint32, _c.c_int, _c.c_int64
+    for name in ("orc_p32_add", "orc_p32_sub", "orc_p32_mul", "orc_p32_div"):
+        getattr(lib, name).argtypes = [u32, u32]
+        getattr(lib, name).restype = u32
+    for name in ("orc_p32_sqrt", "orc_p32_neg", "orc_p32_abs"):
+        getattr(lib, name).argtypes = [u32]
+        getattr(lib, name).restype = u32
+    lib.orc_p32_from_double.argtypes = [_c.c_double]
+    lib.orc_p32_from_double.restype = u32
+    lib.orc_p32_to_double.argtypes = [u32]
+    lib.orc_p32_to_double.restype = _c.c_double
+    for name in ("orc_p32_add_n", "orc_p32_mul_n", "orc_p32_div_n"):
+        getattr(lib, name).argtypes = [_U32P, _U32P, _U32P, i64]
+    lib.orc_p32_sqrt_n.argtypes = [_U32P, _U32P, i64]
+    lib.orc_p32_from_double_n.argtypes = [_F64P, _U32P, i64]
+    lib.orc_p32_to_double_n.argtypes = [_U32P, _F64P, i64]
+    gemm_args = [_c.c_char, _c.c_char, i32, i32, i32, u32, _U32P, i32, _U32P, i32, u32, _U32P, i32]
+    lib.orc_rgemm.argtypes = gemm_args
+    lib.orc_rgemm.restype = i32
+    lib.orc_rgemm_cols.argtypes = gemm_args + [i32, i32]
+    lib.orc_rgemm_cols.restype = i32
+    lib.orc_num_threads.restype = i32
+    lib.orc_iramax.argtypes = [i32, _U32P, i32]
+    lib.orc_iramax.restype = i32
+    lib.orc_rtrsm.argtypes = [_c.c_char] * 4 + [i32, i32, u32, _U32P, i32, _U32P, i32]
+    lib.orc_rtrsm.restype = i32
+    lib.orc_rsyrk.argtypes = [_c.c_char, _c.c_char, i32, i32, u32, _U32P, i32, u32, _U32P, i32]
+    lib.orc_rsyrk.restype = i32
+    lib.orc_rgemv.argtypes = [_c.c_char, i32, i32, u32, _U32P, i32, _U32P, i32, u32, _U32P, i32]
+    lib.orc_rgemv.restype = i32
+    lib.orc_rgetrf.argtypes = [i32, i32, _U32P, i32, _I32P, i32]
+    lib.orc_rgetrf.restype = i32
+    lib.orc_rgetrf2.argtypes = [i32, i32, _U32P, i32, _I32P]
+    lib.orc_rgetrf2.restype = i32
+    lib.orc_rgetrs.argtypes = [_c.c_char, i32, i32, _U32P, i32, _I32P, _U32P, i32]
+    lib.orc_rgetrs.restype = i32
+    lib.orc_rpotrf.argtypes = [_c.c_char, i32, _U32P, i32, i32]
+    lib.orc_rpotrf.restype = i32
+    lib.orc_rpotrf2.argtypes = [_c.c_char, i32, _U32P, i32]
+    lib.orc_rpotrf2.restype = i32
+    lib.orc_rpotrs.argtypes = [_c.c_char, i32, i32, _U32P, i32, _U32P, i32]
+    lib.orc_rpotrs.restype = i32
+    return lib
+
+
+def _load_ref():
+    path = os.path.join(HERE, "_ref", "libposit_ref.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    u32, i32, i64 = _c.c_uint32, _c.c_int, _c.c_int64
+    lib.ref_p32_add.argtypes = [u32, u32]
+    lib.ref_p32_add.restype = u32
+    lib.ref_p32_mul.argtypes = [u32, u32]
+    lib.ref_p32_mul.restype = u32
+    lib.ref_p32_add_n.argtypes = [_U32P, _U32P, _U32P, i64]
+    lib.ref_p32_mul_n.argtypes = [_U32P, _U32P, _U32P, i64]
+    lib.ref_set_nb.argtypes = [i32]
+    lib.ref_rgemm.argtypes = [_c.c_char, _c.c_char, i32, i32, i32, u32, _U32P, i32, _U32P, i32, u32, _U32P, i32]
+    lib.ref_rsyrk.argtypes = [_c.c_char, _c.c_char, i32, i32, u32, _U32P, i32, u32, _U32P, i32]
+    lib.ref_rtrsm.argtypes = [_c.c_char] * 4 + [i32, i32, u32, _U32P, i32, _U32P, i32]
+    lib.ref_rgemv.argtypes = [_c.c_char, i32, i32, u32, _U32P, i32, _U32P, i32, u32, _U32P, i32]
+    lib.ref_iramax.argtypes = [i32, _U32P, i32]
+    lib.ref_iramax.restype = i32
+    lib.ref_rgetrf.argtypes = [i32, i32, _U32P, i32, _I32P, i32]
+    lib.ref_rgetrf.restype = i32
+    lib.ref_rgetrs.argtypes = [_c.c_char, i32, i32, _U32P, i32, _I32P, _U32P, i32]
+    lib.ref_rgetrs.restype = i32
+    lib.ref_rpotrf.argtypes = [_c.c_char, i32, _U32P, i32, i32]
+    lib.ref_rpotrf.restype = i32
+    lib.ref_rpotrs.argtypes = [_c.c_char, i32, i32, _U32P, i32, _U32P, i32]
+    lib.ref_rpotrs.restype = i32
+    return lib
+
+
+orc = _load_orc()
+ref = _load_ref()
+
+P32_ONE = 0x40000000
+P32_NAR = 0x80000000
+P32_MINUS_ONE = 0xC0000000
+
+
+def from_double(x):
+    """float64 array -> posit32 patterns (correctly rounded; unpinned vs SoftPosit)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(x.shape, dtype=np.uint32)
+    orc.orc_p32_from_double_n(x.reshape(-1), out.reshape(-1), x.size)
+    return out
+
+
+def to_double(u):
+    u = np.ascontiguousarray(u, dtype=np.uint32)
+    out = np.empty(u.shape, dtype=np.float64)
+    orc.orc_p32_to_double_n(u.reshape(-1), out.reshape(-1), u.size)
+    return out
+
+
+def p32(x):
+    """One double -> posit32 pattern."""
+    return int(orc.orc_p32_from_double(float(x)))
+
+
+def rgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cols=None):
+    """Oracle Rgemm on flat column-major uint32 buffers; C updated in place.
+    ``cols=(j0, j1)`` restricts the work to those columns of C."""
+    args = (ta.encode(), tb.encode(), m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+    if cols is None:
+        return orc.orc_rgemm(*args)
+    return orc.orc_rgemm_cols(*args, cols[0], cols[1])

@@ -1,0 +1,129 @@
+"""posit_gpu_b200 -- bit-exact posit32 BLAS on B200 (sm_100a).
+
+Host-side mirror of the reference's GPU GEMM interface (libRpack/mpblas_posit.h:49-55,
+libRpack/def.h:63):
+
+    initOpenCL()                      -> init()
+    RgemmG(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+                                      -> Rgemm / RgemmG (host numpy buffers, synchronous)
+    (device-resident form)            -> Rgemm_dev (torch CUDA tensors, stream-ordered)
+
+posit32 values are their raw 32-bit patterns: ``alpha``/``beta`` are ints, matrices are
+flat column-major ``numpy.uint32`` arrays (or any buffer of 4-byte elements) indexed as
+``A[i + j*lda]``.  Errors are raised, never turned into a CPU fallback: an illegal
+argument raises ``ValueError`` carrying the BLAS info code the reference's Mxerbla
+would print, a CUDA failure raises ``RuntimeError``, and a missing library raises
+``ImportError`` at import time.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libposit_gpu_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python posit_gpu_b200/build.py` "
+        "(there is no CPU fallback)")
+
+_lib = ctypes.CDLL(LIB_PATH)
+_c = ctypes
+_VP = _c.c_void_p
+_GEMM_HEAD = [_c.c_char, _c.c_char, _c.c_int, _c.c_int, _c.c_int, _c.c_uint32, _VP, _c.c_int,
+              _VP, _c.c_int, _c.c_uint32, _VP, _c.c_int]
+_lib.posit_init.restype = _c.c_int
+_lib.posit_rgemm.argtypes = _GEMM_HEAD
+_lib.posit_rgemm.restype = _c.c_int
+_lib.posit_rgemm_dev.argtypes = _GEMM_HEAD + [_VP, _c.c_size_t, _VP]
+_lib.posit_rgemm_dev.restype = _c.c_int
+_lib.posit_rgemm_workspace_size.argtypes = [_c.c_char, _c.c_char, _c.c_int, _c.c_int, _c.c_int]
+_lib.posit_rgemm_workspace_size.restype = _c.c_size_t
+_lib.posit_device_error.argtypes = [_c.c_int]
+_lib.posit_device_error.restype = _c.c_int
+_lib.posit_last_cuda_error.restype = _c.c_int
+_lib.posit_strerror.argtypes = [_c.c_int]
+_lib.posit_strerror.restype = _c.c_char_p
+
+P32_ZERO = 0x00000000
+P32_ONE = 0x40000000
+P32_MINUS_ONE = 0xC0000000
+P32_NAR = 0x80000000
+
+
+class PositError(RuntimeError):
+    pass
+
+
+def _check(rc, name):
+    if rc == 0:
+        return
+    if rc > 0:
+        # Mxerbla.cpp:70-73 prints this and exits; here it is an exception
+        raise ValueError(f" ** On entry to {name} parameter number {rc:2d} had an illegal value")
+    msg = _lib.posit_strerror(rc).decode()
+    raise PositError(f"{name}: {msg} (code {rc}, cuda error {_lib.posit_last_cuda_error()})")
+
+
+def _char(c):
+    if isinstance(c, (bytes, bytearray)):
+        c = c.decode()
+    return str(c)[:1].encode() or b" "
+
+
+def _host_ptr(x):
+    if isinstance(x, np.ndarray):
+        if x.dtype.itemsize != 4:
+            raise TypeError("posit32 buffers hold 4-byte elements")
+        if not x.flags.c_contiguous and not x.flags.f_contiguous:
+            raise TypeError("buffer must be contiguous")
+        return x.ctypes.data
+    raise TypeError("host buffers must be numpy arrays of 4-byte elements")
+
+
+def init():
+    """Select the current device and create its context (replaces initOpenCL)."""
+    _check(_lib.posit_init(), "init")
+
+
+initOpenCL = init
+
+
+def Rgemm(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+    """C <- alpha*op(A)*op(B) + beta*C on host buffers, bit-identical to the CPU Rgemm
+    (libRpack/Rgemm.cpp:62-251) for every transpose case.  Synchronous; C in place."""
+    _check(_lib.posit_rgemm(_char(transa), _char(transb), m, n, k, int(alpha) & 0xFFFFFFFF,
+                            _host_ptr(A), lda, _host_ptr(B), ldb, int(beta) & 0xFFFFFFFF,
+                            _host_ptr(C), ldc), "Rgemm ")
+
+
+RgemmG = Rgemm
+
+
+def workspace_size(transa, transb, m, n, k):
+    return int(_lib.posit_rgemm_workspace_size(_char(transa), _char(transb), m, n, k))
+
+
+def Rgemm_dev(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace=None,
+              stream=None):
+    """Device-resident Rgemm: A, B, C (and the optional workspace) are CUDA tensors of a
+    4-byte dtype (raw posit patterns); enqueued on ``stream`` (default: torch's current
+    stream); returns without synchronising."""
+    import torch
+
+    for t in (A, B, C):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.element_size() == 4):
+            raise TypeError("Rgemm_dev takes CUDA tensors of 4-byte elements")
+    if stream is None:
+        stream = torch.cuda.current_stream(C.device)
+    ws_ptr, ws_bytes = None, 0
+    if workspace is not None:
+        ws_ptr, ws_bytes = workspace.data_ptr(), workspace.numel() * workspace.element_size()
+    _check(_lib.posit_rgemm_dev(_char(transa), _char(transb), m, n, k, int(alpha) & 0xFFFFFFFF,
+                                A.data_ptr(), lda, B.data_ptr(), ldb, int(beta) & 0xFFFFFFFF,
+                                C.data_ptr(), ldc, ws_ptr, ws_bytes, stream.cuda_stream), "Rgemm ")
+
+
+def device_error(clear=True):
+    return int(_lib.posit_device_error(1 if clear else 0))

@@ -1,0 +1,226 @@
+// capi.cu -- the C ABI declared in include/posit_gpu.h.
+#include "../../include/posit_gpu.h"
+#include "gemm.cuh"
+#include "posit32.cuh"
+
+#include <atomic>
+#include <ctype.h>
+#include <mutex>
+
+namespace {
+
+std::atomic<int> g_last_cuda_error{0};
+std::once_flag g_pool_once;
+
+int cuda_fail(cudaError_t e)
+{
+    g_last_cuda_error.store((int)e);
+    if (e == cudaErrorMemoryAllocation)
+        return POSIT_E_NO_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return POSIT_E_NO_DEVICE;
+    return POSIT_E_CUDA;
+}
+
+#define PG_TRY(expr)                                                                                       \
+    do {                                                                                                   \
+        cudaError_t e_ = (expr);                                                                           \
+        if (e_ != cudaSuccess)                                                                             \
+            return cuda_fail(e_);                                                                          \
+    } while (0)
+
+bool same(char a, char b) { return toupper((unsigned char)a) == toupper((unsigned char)b); }
+int imax(int a, int b) { return a > b ? a : b; }
+
+// Rgemm.cpp:90-128: argument checks in the reference's order.
+int check_args(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, bool &nota, bool &notb)
+{
+    nota = same(ta, 'N');
+    notb = same(tb, 'N');
+    int nrowa = nota ? m : k, nrowb = notb ? k : n;
+    if (!nota && !same(ta, 'C') && !same(ta, 'T'))
+        return 1;
+    if (!notb && !same(tb, 'C') && !same(tb, 'T'))
+        return 2;
+    if (m < 0)
+        return 3;
+    if (n < 0)
+        return 4;
+    if (k < 0)
+        return 5;
+    if (lda < imax(1, nrowa))
+        return 8;
+    if (ldb < imax(1, nrowb))
+        return 10;
+    if (ldc < imax(1, m))
+        return 13;
+    return 0;
+}
+
+// Keep stream-ordered allocations cached in the device's default pool instead of
+// returning them to the driver at every synchronisation.
+void init_pool()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+}
+
+int ensure_init()
+{
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return e != cudaSuccess ? cuda_fail(e) : POSIT_E_NO_DEVICE;
+    std::call_once(g_pool_once, init_pool);
+    return 0;
+}
+
+// Device-side body shared by both entry points (arguments already checked).
+int rgemm_device(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A, int lda,
+                 const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *ws, size_t ws_bytes,
+                 cudaStream_t st)
+{
+    // quick returns and alpha == 0 (Rgemm.cpp:134-157)
+    if (m == 0 || n == 0 || ((alpha == 0 || k == 0) && beta == pg::P32_ONE))
+        return 0;
+    if (alpha == 0 || k == 0) {
+        // k == 0 leaves beta*C (NN/NT scale C, TN/TT form alpha*0 + beta*C == beta*C)
+        PG_TRY(pg::scale_launch(m, n, beta, C, ldc, st));
+        return 0;
+    }
+    size_t need = pg::gemm_workspace_bytes(m, n, k);
+    bool own = false;
+    if (ws == nullptr) {
+        PG_TRY(cudaMallocAsync(&ws, need, st));
+        own = true;
+    } else if (ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 15u)) {
+        return POSIT_E_WORKSPACE;
+    }
+    cudaError_t e = pg::gemm_launch(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, ws, st);
+    if (own)
+        cudaFreeAsync(ws, st);
+    if (e != cudaSuccess)
+        return cuda_fail(e);
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int posit_init(void)
+{
+    int r = ensure_init();
+    if (r)
+        return r;
+    PG_TRY(cudaFree(nullptr)); // create the context
+    return 0;
+}
+
+size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
+{
+    (void)transa;
+    (void)transb;
+    if (m <= 0 || n <= 0 || k <= 0)
+        return 0;
+    return pg::gemm_workspace_bytes(m, n, k);
+}
+
+int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                    int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *workspace,
+                    size_t workspace_bytes, void *stream)
+{
+    bool nota, notb;
+    int info = check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
+    if (info)
+        return info;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : cudaStreamPerThread;
+    return rgemm_device(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, workspace_bytes, st);
+}
+
+int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, const uint32_t *A, int lda,
+                const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc)
+{
+    bool nota, notb;
+    int info = check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
+    if (info)
+        return info;
+    if (m == 0 || n == 0 || ((alpha == 0 || k == 0) && beta == pg::P32_ONE))
+        return 0;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = cudaStreamPerThread;
+    const bool need_ab = !(alpha == 0 || k == 0);
+    // device copies of exactly the referenced submatrices, packed (ld = rows)
+    const int ar = nota ? m : k, ac = nota ? k : m;
+    const int br = notb ? k : n, bc = notb ? n : k;
+    uint32_t *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    PG_TRY(cudaMallocAsync((void **)&dC, (size_t)m * n * 4, st));
+    if (need_ab) {
+        PG_TRY(cudaMallocAsync((void **)&dA, (size_t)ar * ac * 4, st));
+        PG_TRY(cudaMallocAsync((void **)&dB, (size_t)br * bc * 4, st));
+        PG_TRY(cudaMemcpy2DAsync(dA, (size_t)ar * 4, A, (size_t)lda * 4, (size_t)ar * 4, ac,
+                                 cudaMemcpyHostToDevice, st));
+        PG_TRY(cudaMemcpy2DAsync(dB, (size_t)br * 4, B, (size_t)ldb * 4, (size_t)br * 4, bc,
+                                 cudaMemcpyHostToDevice, st));
+    }
+    if (beta != 0) // with beta == 0 the reference never reads C (Rgemm.cpp:143-147, 170-173, 197-198)
+        PG_TRY(cudaMemcpy2DAsync(dC, (size_t)m * 4, C, (size_t)ldc * 4, (size_t)m * 4, n,
+                                 cudaMemcpyHostToDevice, st));
+    int rc = rgemm_device(nota, notb, m, n, k, alpha, dA, ar, dB, br, beta, dC, m, nullptr, 0, st);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(C, (size_t)ldc * 4, dC, (size_t)m * 4, (size_t)m * 4, n,
+                                          cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(e);
+    }
+    if (dA)
+        cudaFreeAsync(dA, st);
+    if (dB)
+        cudaFreeAsync(dB, st);
+    cudaFreeAsync(dC, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == 0 && e != cudaSuccess)
+        rc = cuda_fail(e);
+    if (rc == 0 && pg::read_device_error(true) != 0)
+        rc = POSIT_E_DEVICE_FAULT;
+    return rc;
+}
+
+int posit_device_error(int clear) { return pg::read_device_error(clear != 0); }
+
+int posit_last_cuda_error(void) { return g_last_cuda_error.load(); }
+
+const char *posit_strerror(int code)
+{
+    switch (code) {
+    case 0:
+        return "success";
+    case POSIT_E_CUDA:
+        return "CUDA runtime error";
+    case POSIT_E_NO_DEVICE:
+        return "no usable CUDA device";
+    case POSIT_E_NO_MEMORY:
+        return "out of device memory";
+    case POSIT_E_DEVICE_FAULT:
+        return "kernel error flag raised (bounded wait expired)";
+    case POSIT_E_WORKSPACE:
+        return "workspace too small or misaligned";
+    default:
+        if (code > 0)
+            return "illegal argument (BLAS info = parameter number)";
+        return "unknown error";
+    }
+}
+
+} // extern "C"

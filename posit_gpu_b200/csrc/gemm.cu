@@ -1,0 +1,382 @@
+// gemm.cu -- bit-exact posit32 GEMM for sm_100a.
+//
+// Reproduces the per-element operation order of the reference CPU Rgemm
+// (libRpack/Rgemm.cpp:163-247):
+//   NN / NT  "scale, then accumulate":  c <- beta*c (0 if beta == 0, untouched if
+//            beta == 1), then c <- c + (alpha*b_lj)*a_il for l = 0..k-1;
+//   TN / TT  "dot, then combine":       t <- 0, t <- t + a_li*b_lj for l = 0..k-1,
+//            then c <- alpha*t (beta == 0) or alpha*t + beta*c.
+// Both are one chain of "acc <- acc + x_l*y_l" per output; they differ only in the
+// operand prescale (alpha*B for NN/NT), the accumulator's start value and the
+// epilogue.  So one main kernel serves all four transpose cases:
+//
+//  1. decode pre-pass: op(A) and op(B) (times alpha for NN/NT, rounded exactly as the
+//     reference rounds alpha*b_lj) are decoded ONCE per element into
+//     (scale, significand|sign) pairs, stored tile-contiguously in a workspace:
+//     A as [m-tile][k-tile][l][i], B as [n-tile][k-tile][l][j].  Transposition is
+//     absorbed here, so the main kernel never sees lda/ldb.
+//  2. main kernel: one CTA per 64x64 tile of C, 256 threads, 4x4 outputs per thread
+//     held in decoded form across the whole k loop.  Each 16-deep k tile of A and B
+//     (8 KB each) is brought into shared memory by the bulk-copy (TMA) engine
+//     (cp.async.bulk + mbarrier transaction counts, 3 stages).  The inner step is
+//     integer-only and branch-free; the rare step that leaves the fast range (long
+//     regimes, zero or NaR operands, exact cancellation) is redone exactly afterwards.
+#include "gemm.cuh"
+#include "posit32.cuh"
+
+namespace pg {
+
+__device__ int g_dev_error;
+
+// ---------------------------------------------------------------------------
+// PTX helpers: mbarrier + bulk async copy (TMA engine, no multicast)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+// Every wait is bounded: a copy that never lands turns into an error flag, not a hang.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 24); ++it)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Decoded element packing: {scale, significand | sign << 31}
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint2 pack_dp(const dp32 &d)
+{
+    return make_uint2((uint32_t)d.s, d.g | (d.x << 31));
+}
+
+__device__ __forceinline__ dp32 unpack_dp(uint32_t s, uint32_t gx)
+{
+    dp32 d;
+    d.s = (int32_t)s;
+    d.g = gx & 0x7FFFFFFFu;
+    d.x = gx >> 31;
+    return d;
+}
+
+GemmPlan gemm_plan(int m, int n, int k)
+{
+    GemmPlan p;
+    p.m = m;
+    p.n = n;
+    p.k = k;
+    p.mt = (m + BM - 1) / BM;
+    p.nt = (n + BN - 1) / BN;
+    p.kt = (k + BK - 1) / BK;
+    p.a_bytes = (size_t)p.mt * p.kt * BK * BM * sizeof(uint2);
+    p.b_bytes = (size_t)p.nt * p.kt * BK * BN * sizeof(uint2);
+    return p;
+}
+
+size_t gemm_workspace_bytes(int m, int n, int k)
+{
+    GemmPlan p = gemm_plan(m, n, k);
+    return p.a_bytes + p.b_bytes;
+}
+
+// ---------------------------------------------------------------------------
+// Decode pre-pass
+// ---------------------------------------------------------------------------
+// op(A) (m x k) -> Ad[mt][kt][l][i].  Rows/columns beyond the matrix hold 1.0 so that
+// padded lanes stay on the fast path; their results are never stored.
+__global__ void decode_a_kernel(bool nota, int m, int k, const uint32_t *__restrict__ A, size_t lda,
+                                int KT, size_t total, uint2 *__restrict__ Ad)
+{
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(idx % BM);
+        size_t r = idx / BM;
+        int l = (int)(r % BK);
+        r /= BK;
+        int kt = (int)(r % KT);
+        int mt = (int)(r / KT);
+        int row = mt * BM + i, kk = kt * BK + l;
+        uint32_t u = P32_ONE;
+        if (row < m && kk < k)
+            u = nota ? A[(size_t)row + (size_t)kk * lda] : A[(size_t)kk + (size_t)row * lda];
+        Ad[idx] = pack_dp(decode(u));
+    }
+}
+
+// op(B) (k x n) -> Td[nt][kt][l][j], times alpha (exactly rounded) when `scale`.
+__global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restrict__ B, size_t ldb,
+                                bool scale, uint32_t alpha, int KT, size_t total, uint2 *__restrict__ Td)
+{
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        int j = (int)(idx % BN);
+        size_t r = idx / BN;
+        int l = (int)(r % BK);
+        r /= BK;
+        int kt = (int)(r % KT);
+        int nt = (int)(r / KT);
+        int col = nt * BN + j, kk = kt * BK + l;
+        uint32_t u = P32_ONE;
+        if (col < n && kk < k) {
+            u = notb ? B[(size_t)kk + (size_t)col * ldb] : B[(size_t)col + (size_t)kk * ldb];
+            if (scale)
+                u = pmul(alpha, u); // Rgemm.cpp:180 / 222: temp = alpha*b
+        }
+        Td[idx] = pack_dp(decode(u));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Main kernel
+// ---------------------------------------------------------------------------
+// Thread (tx, ty) owns rows {2tx, 2tx+1, 32+2tx, 33+2tx} and the same pattern of
+// columns with ty: the 16-byte shared-memory loads of a warp then hit distinct banks.
+__device__ __forceinline__ int own_off(int t, int q) { return (q >> 1) * 32 + 2 * t + (q & 1); }
+
+template <bool DOT>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    gemm_main_kernel(int m, int n, int k, int KT, uint32_t alpha, uint32_t beta,
+                     const uint2 *__restrict__ Ad, const uint2 *__restrict__ Td, uint32_t *__restrict__ C,
+                     size_t ldc)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint2 *As = reinterpret_cast<uint2 *>(smem_raw);
+    uint2 *Ts = As + STAGES * BK * BM;
+    __shared__ __align__(8) uint64_t full[STAGES];
+
+    const int tid = threadIdx.x;
+    const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+    const int mt = blockIdx.x, nt = blockIdx.y;
+    const uint2 *Ablk = Ad + (size_t)mt * KT * BK * BM;
+    const uint2 *Tblk = Td + (size_t)nt * KT * BK * BN;
+    constexpr uint32_t kTileBytes = BK * BM * sizeof(uint2);
+    static_assert(BM == BN, "one tile size for both operands");
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s)
+            mbar_init(&full[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < STAGES && s < KT; ++s) {
+            mbar_arrive_expect_tx(&full[s], 2 * kTileBytes);
+            bulk_g2s(As + s * BK * BM, Ablk + (size_t)s * BK * BM, kTileBytes, &full[s]);
+            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)s * BK * BN, kTileBytes, &full[s]);
+        }
+    }
+
+    // Accumulators: NN/NT start from beta*C, TN/TT from zero.
+    dp32 acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int row = mt * BM + own_off(tx, i), col = nt * BN + own_off(ty, j);
+            uint32_t u = 0;
+            if (!DOT) {
+                u = P32_ONE;
+                if (row < m && col < n) {
+                    u = C[(size_t)row + (size_t)col * ldc];
+                    if (beta == 0)
+                        u = 0; // Rgemm.cpp:170-173: C is not read
+                    else if (beta != P32_ONE)
+                        u = pmul(beta, u);
+                }
+            }
+            acc[i][j] = decode(u);
+        }
+    }
+
+    bool bad = false;
+    int kt_stop = 0;
+    for (int kt = 0; kt < KT; ++kt) {
+        kt_stop = kt;
+        const int s = kt % STAGES;
+        const uint32_t parity = (uint32_t)(kt / STAGES) & 1u;
+        const bool arrived = mbar_wait_bounded(&full[s], parity);
+        const uint2 *as = As + s * BK * BM;
+        const uint2 *ts = Ts + s * BK * BN;
+        const int lmax = min(BK, k - kt * BK);
+        for (int l = 0; l < lmax; ++l) {
+            const uint4 a01 = *reinterpret_cast<const uint4 *>(as + l * BM + 2 * tx);
+            const uint4 a23 = *reinterpret_cast<const uint4 *>(as + l * BM + 32 + 2 * tx);
+            const uint4 t01 = *reinterpret_cast<const uint4 *>(ts + l * BN + 2 * ty);
+            const uint4 t23 = *reinterpret_cast<const uint4 *>(ts + l * BN + 32 + 2 * ty);
+            dp32 a[TM], t[TN];
+            a[0] = unpack_dp(a01.x, a01.y);
+            a[1] = unpack_dp(a01.z, a01.w);
+            a[2] = unpack_dp(a23.x, a23.y);
+            a[3] = unpack_dp(a23.z, a23.w);
+            t[0] = unpack_dp(t01.x, t01.y);
+            t[1] = unpack_dp(t01.z, t01.w);
+            t[2] = unpack_dp(t23.x, t23.y);
+            t[3] = unpack_dp(t23.z, t23.w);
+            uint32_t fail = 0;
+#pragma unroll
+            for (int i = 0; i < TM; ++i) {
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    dp32 p, r;
+                    bool ok = dmul_fast(t[j], a[i], p);
+                    ok = dadd_fast(acc[i][j], p, r) && ok;
+                    if (ok)
+                        acc[i][j] = r;
+                    else
+                        fail |= 1u << (i * TN + j);
+                }
+            }
+            if (fail) { // rare: redo the failed steps exactly, in the same order
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j)
+                        if (fail & (1u << (i * TN + j)))
+                            acc[i][j] = dmac_exact(acc[i][j], t[j], a[i]);
+            }
+        }
+        // every thread is done with stage s before it is refilled
+        bad = __syncthreads_or(!arrived) != 0;
+        if (bad)
+            break;
+        if (tid == 0 && kt + STAGES < KT) {
+            const int nk = kt + STAGES;
+            mbar_arrive_expect_tx(&full[s], 2 * kTileBytes);
+            bulk_g2s(As + s * BK * BM, Ablk + (size_t)nk * BK * BM, kTileBytes, &full[s]);
+            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)nk * BK * BN, kTileBytes, &full[s]);
+        }
+    }
+
+    if (bad) {
+        if (tid == 0) {
+            atomicOr(&g_dev_error, DEV_ERR_WAIT_TIMEOUT);
+            // let copies already in flight land before the CTA's shared memory goes away
+            for (int q = kt_stop + 1; q < KT && q < kt_stop + STAGES; ++q)
+                (void)mbar_wait_bounded(&full[q % STAGES], (uint32_t)(q / STAGES) & 1u);
+        }
+        return;
+    }
+
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int row = mt * BM + own_off(tx, i), col = nt * BN + own_off(ty, j);
+            if (row < m && col < n) {
+                uint32_t *cp = C + (size_t)row + (size_t)col * ldc;
+                uint32_t v = encode(acc[i][j]);
+                if (DOT) { // Rgemm.cpp:197-201
+                    uint32_t at = pmul(alpha, v);
+                    v = (beta == 0) ? at : padd(at, pmul(beta, *cp));
+                }
+                *cp = v;
+            }
+        }
+    }
+}
+
+__global__ void scale_kernel(int m, int n, uint32_t beta, uint32_t *__restrict__ C, size_t ldc)
+{
+    size_t total = (size_t)m * n;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        size_t i = idx % m, j = idx / m;
+        uint32_t *cp = C + i + j * ldc;
+        *cp = (beta == 0) ? 0u : pmul(beta, *cp); // Rgemm.cpp:142-156
+    }
+}
+
+static int grid_for(size_t total, int threads)
+{
+    size_t b = (total + threads - 1) / threads;
+    size_t cap = 148 * 16;
+    return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                        int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
+                        void *workspace, cudaStream_t stream)
+{
+    GemmPlan p = gemm_plan(m, n, k);
+    uint2 *Ad = reinterpret_cast<uint2 *>(workspace);
+    uint2 *Td = reinterpret_cast<uint2 *>(reinterpret_cast<unsigned char *>(workspace) + p.a_bytes);
+    const bool dot = !nota; // TN / TT use the dot-then-combine order
+    size_t na = p.a_bytes / sizeof(uint2), nb = p.b_bytes / sizeof(uint2);
+    decode_a_kernel<<<grid_for(na, 256), 256, 0, stream>>>(nota, m, k, A, (size_t)lda, p.kt, na, Ad);
+    decode_b_kernel<<<grid_for(nb, 256), 256, 0, stream>>>(notb, k, n, B, (size_t)ldb, !dot, alpha, p.kt, nb,
+                                                           Td);
+    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2);
+    dim3 grid(p.mt, p.nt);
+    cudaError_t e;
+    if (dot) {
+        e = cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        gemm_main_kernel<true><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
+    } else {
+        e = cudaFuncSetAttribute(gemm_main_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        gemm_main_kernel<false><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream)
+{
+    scale_kernel<<<grid_for((size_t)m * n, 256), 256, 0, stream>>>(m, n, beta, C, (size_t)ldc);
+    return cudaGetLastError();
+}
+
+int read_device_error(bool clear)
+{
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_dev_error, sizeof(int)) != cudaSuccess)
+        return -1;
+    if (clear && v) {
+        int z = 0;
+        cudaMemcpyToSymbol(g_dev_error, &z, sizeof(int));
+    }
+    return v;
+}
+
+} // namespace pg

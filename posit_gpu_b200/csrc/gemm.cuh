@@ -1,0 +1,41 @@
+// gemm.cuh -- posit32 GEMM kernels for sm_100a (declarations shared by the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pg {
+
+// Output tile of one CTA and the k-depth of one staged tile.
+constexpr int BM = 64;
+constexpr int BN = 64;
+constexpr int BK = 16;
+constexpr int TM = 4; // rows per thread
+constexpr int TN = 4; // columns per thread
+constexpr int NTHREADS = (BM / TM) * (BN / TN);
+constexpr int STAGES = 3;
+
+// Error flags a kernel can raise (read back with posit_get_device_error).
+constexpr int DEV_ERR_WAIT_TIMEOUT = 1;
+
+struct GemmPlan {
+    int m, n, k;
+    int mt, nt, kt; // tile counts
+    size_t a_bytes, b_bytes;
+};
+
+GemmPlan gemm_plan(int m, int n, int k);
+size_t gemm_workspace_bytes(int m, int n, int k);
+
+// Decode op(A) and alpha*op(B) (or op(B) for the dot-then-combine order) into the
+// workspace, then run the main kernel.  Device pointers; stream-ordered.
+cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alpha,
+                        const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
+                        uint32_t *C, int ldc, void *workspace, cudaStream_t stream);
+
+// C <- 0 or beta*C on the m x n submatrix (alpha == 0 or k == 0 with beta != 1).
+cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream);
+
+int read_device_error(bool clear);
+
+} // namespace pg
