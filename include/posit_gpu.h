@@ -57,8 +57,23 @@ int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alph
 /* Bytes of device workspace posit_rgemm_dev needs for this shape (0 when none). */
 size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k);
 
+/* Element-wise conversions on device buffers, asynchronous on `stream`.
+ * Replace the SoftPosit class conversions the reference drivers use to build their
+ * inputs and error norms (posit32 = double, main_gemm.cpp:99-104; .toDouble(),
+ * main_gemm.cpp:162-163).  double -> posit32 is correctly rounded (nearest, ties to the
+ * even pattern, never to zero or NaR; NaN/inf -> NaR); posit32 -> double is exact. */
+int posit_from_double_dev(const double *x, uint32_t *out, size_t n, void *stream);
+int posit_to_double_dev(const uint32_t *x, double *out, size_t n, void *stream);
+
 /* Reads (and with clear != 0 resets) the device-side error flags raised by kernels. */
 int posit_device_error(int clear);
+
+/* Instrumentation (no reference counterpart).  When enabled, CUDA events are recorded
+ * around every GEMM main-kernel launch on its own stream; posit_profile_read waits for
+ * them and returns the summed main-kernel time, the number of main-kernel launches and
+ * the number of all kernels this library launched since the last reset. */
+void posit_profile_enable(int on);
+int posit_profile_read(double *main_kernel_ms, long long *main_launches, long long *all_launches, int reset);
 
 /* The last CUDA error code seen by the library (cudaError_t value). */
 int posit_last_cuda_error(void);

@@ -43,6 +43,13 @@ _lib.posit_rgemm_workspace_size.restype = _c.c_size_t
 _lib.posit_device_error.argtypes = [_c.c_int]
 _lib.posit_device_error.restype = _c.c_int
 _lib.posit_last_cuda_error.restype = _c.c_int
+_lib.posit_profile_enable.argtypes = [_c.c_int]
+_lib.posit_profile_read.argtypes = [_c.POINTER(_c.c_double), _c.POINTER(_c.c_longlong),
+                                    _c.POINTER(_c.c_longlong), _c.c_int]
+_lib.posit_from_double_dev.argtypes = [_VP, _VP, _c.c_size_t, _VP]
+_lib.posit_from_double_dev.restype = _c.c_int
+_lib.posit_to_double_dev.argtypes = [_VP, _VP, _c.c_size_t, _VP]
+_lib.posit_to_double_dev.restype = _c.c_int
 _lib.posit_strerror.argtypes = [_c.c_int]
 _lib.posit_strerror.restype = _c.c_char_p
 
@@ -125,5 +132,43 @@ def Rgemm_dev(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, work
                                 C.data_ptr(), ldc, ws_ptr, ws_bytes, stream.cuda_stream), "Rgemm ")
 
 
+def from_double_dev(x, out=None, stream=None):
+    """float64 CUDA tensor -> posit32 patterns (int32 CUDA tensor), correctly rounded."""
+    import torch
+    if not (x.is_cuda and x.dtype == torch.float64 and x.is_contiguous()):
+        raise TypeError("from_double_dev takes a contiguous float64 CUDA tensor")
+    if out is None:
+        out = torch.empty(x.shape, dtype=torch.int32, device=x.device)
+    stream = stream or torch.cuda.current_stream(x.device)
+    _check(_lib.posit_from_double_dev(x.data_ptr(), out.data_ptr(), x.numel(), stream.cuda_stream),
+           "from_double")
+    return out
+
+
+def to_double_dev(u, out=None, stream=None):
+    """posit32 patterns (4-byte CUDA tensor) -> float64 CUDA tensor (exact)."""
+    import torch
+    if not (u.is_cuda and u.element_size() == 4 and u.is_contiguous()):
+        raise TypeError("to_double_dev takes a contiguous 4-byte CUDA tensor")
+    if out is None:
+        out = torch.empty(u.shape, dtype=torch.float64, device=u.device)
+    stream = stream or torch.cuda.current_stream(u.device)
+    _check(_lib.posit_to_double_dev(u.data_ptr(), out.data_ptr(), u.numel(), stream.cuda_stream),
+           "to_double")
+    return out
+
+
 def device_error(clear=True):
     return int(_lib.posit_device_error(1 if clear else 0))
+
+
+def profile_enable(on=True):
+    """Record CUDA events around every GEMM main-kernel launch (on its stream)."""
+    _lib.posit_profile_enable(1 if on else 0)
+
+
+def profile_read(reset=True):
+    """-> (main-kernel milliseconds, main-kernel launches, all kernel launches)."""
+    ms, mains, alls = _c.c_double(), _c.c_longlong(), _c.c_longlong()
+    _lib.posit_profile_read(_c.byref(ms), _c.byref(mains), _c.byref(alls), 1 if reset else 0)
+    return ms.value, mains.value, alls.value

@@ -197,7 +197,32 @@ int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, c
     return rc;
 }
 
+int posit_from_double_dev(const double *x, uint32_t *out, size_t n, void *stream)
+{
+    int r = ensure_init();
+    if (r)
+        return r;
+    PG_TRY(pg::convert_launch(true, x, out, n, stream ? (cudaStream_t)stream : cudaStreamPerThread));
+    return 0;
+}
+
+int posit_to_double_dev(const uint32_t *x, double *out, size_t n, void *stream)
+{
+    int r = ensure_init();
+    if (r)
+        return r;
+    PG_TRY(pg::convert_launch(false, x, out, n, stream ? (cudaStream_t)stream : cudaStreamPerThread));
+    return 0;
+}
+
 int posit_device_error(int clear) { return pg::read_device_error(clear != 0); }
+
+void posit_profile_enable(int on) { pg::profile_enable(on != 0); }
+
+int posit_profile_read(double *main_kernel_ms, long long *main_launches, long long *all_launches, int reset)
+{
+    return pg::profile_read(main_kernel_ms, main_launches, all_launches, reset != 0);
+}
 
 int posit_last_cuda_error(void) { return g_last_cuda_error.load(); }
 

@@ -24,6 +24,9 @@
 #include "gemm.cuh"
 #include "posit32.cuh"
 
+#include <mutex>
+#include <vector>
+
 namespace pg {
 
 __device__ int g_dev_error;
@@ -325,6 +328,81 @@ __global__ void scale_kernel(int m, int n, uint32_t beta, uint32_t *__restrict__
     }
 }
 
+// ---------------------------------------------------------------------------
+// Instrumentation
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+double g_prof_ms = 0.0;
+long long g_prof_main = 0, g_prof_all = 0;
+
+void prof_count(int launches)
+{
+    if (!g_prof_on)
+        return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_all += launches;
+}
+
+cudaEvent_t prof_mark(cudaStream_t st)
+{
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess)
+        return nullptr;
+    cudaEventRecord(ev, st);
+    return ev;
+}
+} // namespace
+
+void profile_enable(bool on)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_on = on;
+}
+
+int profile_read(double *main_ms, long long *main_launches, long long *all_launches, bool reset)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto &pr : g_prof_events) {
+        float ms = 0.f;
+        if (pr.first && pr.second && cudaEventSynchronize(pr.second) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess)
+            g_prof_ms += ms;
+        if (pr.first)
+            cudaEventDestroy(pr.first);
+        if (pr.second)
+            cudaEventDestroy(pr.second);
+        g_prof_main += 1;
+    }
+    g_prof_events.clear();
+    if (main_ms)
+        *main_ms = g_prof_ms;
+    if (main_launches)
+        *main_launches = g_prof_main;
+    if (all_launches)
+        *all_launches = g_prof_all;
+    if (reset) {
+        g_prof_ms = 0.0;
+        g_prof_main = 0;
+        g_prof_all = 0;
+    }
+    return 0;
+}
+
+__global__ void from_double_kernel(const double *__restrict__ x, uint32_t *__restrict__ out, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = p32_from_double(x[i]);
+}
+
+__global__ void to_double_kernel(const uint32_t *__restrict__ x, double *__restrict__ out, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = p32_to_double(x[i]);
+}
+
 static int grid_for(size_t total, int threads)
 {
     size_t b = (total + threads - 1) / threads;
@@ -346,24 +424,43 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
                                                            Td);
     const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2);
     dim3 grid(p.mt, p.nt);
-    cudaError_t e;
-    if (dot) {
-        e = cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess)
-            return e;
+    cudaError_t e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem)
+                        : cudaFuncSetAttribute(gemm_main_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    const bool prof = g_prof_on;
+    cudaEvent_t e0 = prof ? prof_mark(stream) : nullptr;
+    if (dot)
         gemm_main_kernel<true><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
-    } else {
-        e = cudaFuncSetAttribute(gemm_main_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess)
-            return e;
+    else
         gemm_main_kernel<false><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
+    if (prof) {
+        cudaEvent_t e1 = prof_mark(stream);
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        g_prof_events.emplace_back(e0, e1);
     }
+    prof_count(3);
     return cudaGetLastError();
 }
 
 cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream)
 {
     scale_kernel<<<grid_for((size_t)m * n, 256), 256, 0, stream>>>(m, n, beta, C, (size_t)ldc);
+    prof_count(1);
+    return cudaGetLastError();
+}
+
+cudaError_t convert_launch(bool to_posit, const void *in, void *out, size_t n, cudaStream_t stream)
+{
+    if (n == 0)
+        return cudaSuccess;
+    if (to_posit)
+        from_double_kernel<<<grid_for(n, 256), 256, 0, stream>>>((const double *)in, (uint32_t *)out, n);
+    else
+        to_double_kernel<<<grid_for(n, 256), 256, 0, stream>>>((const uint32_t *)in, (double *)out, n);
+    prof_count(1);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,14 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
 // C <- 0 or beta*C on the m x n submatrix (alpha == 0 or k == 0 with beta != 1).
 cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream);
 
+// Element-wise IEEE double <-> posit32 conversion on device buffers.
+cudaError_t convert_launch(bool to_posit, const void *in, void *out, size_t n, cudaStream_t stream);
+
 int read_device_error(bool clear);
+
+// Optional instrumentation: CUDA events around each main-kernel launch, recorded on
+// the launch stream, plus a count of this library's kernel launches.
+void profile_enable(bool on);
+int profile_read(double *main_ms, long long *main_launches, long long *all_launches, bool reset);
 
 } // namespace pg

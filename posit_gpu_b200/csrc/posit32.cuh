@@ -16,6 +16,7 @@
 //     of the fast path's range test; the caller then redoes that step exactly.
 #pragma once
 #include <stdint.h>
+#include <string.h>
 
 #if defined(__CUDACC__)
 #define PG_HD __host__ __device__ __forceinline__
@@ -298,6 +299,44 @@ PG_HD uint32_t psqrt(uint32_t a)
     uint64_t rem;
     uint64_t r = isqrt64(m << 32, &rem);
     return pack_exact(0, (d.s - odd) / 2, r << 31, rem != 0);
+}
+
+// IEEE double -> posit32, correctly rounded (nearest, ties to even pattern; never to
+// zero or NaR).  SoftPosit's convertDoubleToP32 has no in-tree source: unpinned.
+PG_HD uint32_t p32_from_double(double x)
+{
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    uint32_t neg = (uint32_t)(b >> 63);
+    int32_t ex = (int32_t)((b >> 52) & 0x7FF);
+    uint64_t man = b & 0xFFFFFFFFFFFFFull;
+    if (ex == 0x7FF)
+        return P32_NAR; // inf / nan
+    if (ex == 0) {
+        if (man == 0)
+            return 0;
+        return neg ? 0u - 1u : 1u; // subnormal doubles lie far below minpos
+    }
+    uint64_t sig62 = ((uint64_t)1 << 62) | (man << 10);
+    return pack_exact(neg, ex - 1023, sig62, 0);
+}
+
+// posit32 -> IEEE double (exact).  NaR -> quiet NaN.
+PG_HD double p32_to_double(uint32_t u)
+{
+    uint64_t b;
+    if (u == 0) {
+        b = 0;
+    } else if (u == P32_NAR) {
+        b = 0x7FF8000000000000ull;
+    } else {
+        dp32 d = decode(u);
+        uint64_t man = ((uint64_t)(d.g & 0x3FFFFFFFu)) << 22; // 30 fraction bits -> 52
+        b = ((uint64_t)d.x << 63) | ((uint64_t)(d.s + 1023) << 52) | man;
+    }
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
 }
 
 PG_HD uint32_t pneg(uint32_t a) { return 0u - a; }

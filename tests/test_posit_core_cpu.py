@@ -1,0 +1,102 @@
+"""The product's posit32 arithmetic (the same header the CUDA kernels compile),
+built for the host, against the oracle: pattern-level ops, conversions, and the
+decoded-domain multiply-add fast path of the GEMM inner loop."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+U32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+F64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+@pytest.fixture(scope="module")
+def hc(tmp_path_factory):
+    out = tmp_path_factory.mktemp("hc") / "libhc.so"
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", str(out),
+                           os.path.join(HERE, "host_core_check.cpp")])
+    lib = ctypes.CDLL(str(out))
+    for nm in ("hc_pmul_n", "hc_padd_n", "hc_pdiv_n"):
+        getattr(lib, nm).argtypes = [U32, U32, U32, ctypes.c_long]
+    lib.hc_psqrt_n.argtypes = [U32, U32, ctypes.c_long]
+    lib.hc_from_double_n.argtypes = [F64, U32, ctypes.c_long]
+    lib.hc_dmac_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
+    lib.hc_dmac_n.restype = ctypes.c_long
+    lib.hc_chain.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_long]
+    return lib
+
+
+def _mix(rng, n):
+    """Random patterns, U[-1,1], wide range, long regimes, specials."""
+    parts = [rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32),
+             oracle.from_double(rng.uniform(-1, 1, n)),
+             oracle.from_double((10.0 ** rng.uniform(-20, 20, n)) * np.where(rng.integers(0, 2, n) == 1, -1, 1)),
+             (rng.integers(0, 4096, n).astype(np.uint32) ^ (rng.integers(0, 2, n).astype(np.uint32) * 0x7FFFFFFF)),
+             np.array([0, 0x80000000, 1, 0x7FFFFFFF, 0xFFFFFFFF, 0x80000001, 0x40000000] * (n // 7 + 1),
+                      dtype=np.uint32)[:n]]
+    x = np.concatenate(parts)
+    rng.shuffle(x)
+    return x
+
+
+def test_pattern_ops_match_oracle(hc):
+    rng = np.random.default_rng(1)
+    a, b = _mix(rng, 200_000), _mix(rng, 200_000)
+    for f_hc, f_or in ((hc.hc_pmul_n, oracle.orc.orc_p32_mul_n), (hc.hc_padd_n, oracle.orc.orc_p32_add_n),
+                       (hc.hc_pdiv_n, oracle.orc.orc_p32_div_n)):
+        o1, o2 = np.empty_like(a), np.empty_like(a)
+        f_hc(a, b, o1, a.size)
+        f_or(a, b, o2, a.size)
+        assert np.array_equal(o1, o2), f_hc.__name__
+    o1, o2 = np.empty_like(a), np.empty_like(a)
+    hc.hc_psqrt_n(a, o1, a.size)
+    oracle.orc.orc_p32_sqrt_n(a, o2, a.size)
+    assert np.array_equal(o1, o2)
+
+
+def test_from_double_matches_oracle(hc):
+    rng = np.random.default_rng(2)
+    x = np.concatenate([rng.uniform(-1, 1, 100_000), 10.0 ** rng.uniform(-45, 45, 100_000),
+                        rng.integers(0, 2**63, 100_000, dtype=np.int64).view(np.float64),
+                        [0.0, -0.0, np.inf, -np.inf, np.nan, 5e-324, 1e308]])
+    o1 = np.empty(x.size, np.uint32)
+    hc.hc_from_double_n(x, o1, x.size)
+    assert np.array_equal(o1, oracle.from_double(x))
+
+
+def test_decoded_mac_matches_oracle(hc):
+    rng = np.random.default_rng(3)
+    n = 300_000
+    c, t, a = _mix(rng, n), _mix(rng, n), _mix(rng, n)
+    # near-cancelling accumulators
+    prod = np.empty_like(t)
+    oracle.orc.orc_p32_mul_n(t, a, prod, t.size)
+    sel = rng.integers(0, 9, c.size) == 0
+    c[sel] = ((0 - prod[sel].astype(np.int64) + rng.integers(-3, 4, sel.sum())) & 0xFFFFFFFF).astype(np.uint32)
+    out = np.empty_like(c)
+    fast = hc.hc_dmac_n(c, t, a, out, c.size)
+    want = np.empty_like(c)
+    oracle.orc.orc_p32_add_n(c, prod, want, c.size)
+    assert np.array_equal(out, want)
+    assert fast > 0.5 * c.size
+
+
+def test_decoded_chains_match_oracle(hc):
+    rng = np.random.default_rng(4)
+    nch, ln = 400, 500
+    c0 = oracle.from_double(rng.uniform(-1, 1, nch))
+    t = oracle.from_double(-rng.uniform(-1, 1, nch * ln))
+    a = oracle.from_double(rng.uniform(-1, 1, nch * ln))
+    out = np.empty(nch, np.uint32)
+    hc.hc_chain(c0, t, a, out, nch, ln)
+    want = c0.copy()
+    for l in range(ln):
+        p = np.empty(nch, np.uint32)
+        oracle.orc.orc_p32_mul_n(np.ascontiguousarray(t[l::ln]), np.ascontiguousarray(a[l::ln]), p, nch)
+        oracle.orc.orc_p32_add_n(want, p, want, nch)
+    assert np.array_equal(out, want)
