@@ -25,6 +25,7 @@ extern "C" {
 #define POSIT_E_NO_MEMORY (-3)    /* device or pinned-host allocation failed */
 #define POSIT_E_DEVICE_FAULT (-4) /* a kernel raised its error flag (bounded wait expired) */
 #define POSIT_E_WORKSPACE (-5)    /* caller-provided workspace too small */
+#define POSIT_E_NOALLOC_LIMIT (-6) /* shape needs more scratch than posit_rgemm_dev_noalloc has */
 
 /* Replaces initOpenCL (libRpack/def.h:63, libRpack/Rgemm_opencl.cpp:59-70): selects
  * the current CUDA device, creates its context and warms the kernels.  Optional: every
@@ -53,6 +54,20 @@ int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, c
 int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
                     int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
                     void *workspace, size_t workspace_bytes, void *stream);
+
+/* posit_rgemm_dev for callers that cannot allocate device memory (a host whose memory
+ * manager has reserved the GPU's memory, or a loop that must not let cudaMalloc/cudaFree
+ * synchronise the device).  No counterpart in the reference.  It allocates nothing: its
+ * scratch is a static device array of POSIT_NOALLOC_SCRATCH_BYTES compiled into the
+ * library, held by every GPU that loads the library until the process exits.  Shapes
+ * whose posit_rgemm_workspace_size exceeds that size return POSIT_E_NOALLOC_LIMIT (e.g.
+ * 2048^3 fits exactly; an 8192 x 8192 x 256 trailing update needs 34 MB and fits).
+ * The first call on a device looks up the array's address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+#define POSIT_NOALLOC_SCRATCH_BYTES (64u << 20)
+int posit_rgemm_dev_noalloc(char transa, char transb, int m, int n, int k, uint32_t alpha,
+                            const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
+                            uint32_t *C, int ldc, void *stream);
 
 /* Bytes of device workspace posit_rgemm_dev needs for this shape (0 when none). */
 size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k);

@@ -38,6 +38,8 @@ _lib.posit_rgemm.argtypes = _GEMM_HEAD
 _lib.posit_rgemm.restype = _c.c_int
 _lib.posit_rgemm_dev.argtypes = _GEMM_HEAD + [_VP, _c.c_size_t, _VP]
 _lib.posit_rgemm_dev.restype = _c.c_int
+_lib.posit_rgemm_dev_noalloc.argtypes = _GEMM_HEAD + [_VP]
+_lib.posit_rgemm_dev_noalloc.restype = _c.c_int
 _lib.posit_rgemm_workspace_size.argtypes = [_c.c_char, _c.c_char, _c.c_int, _c.c_int, _c.c_int]
 _lib.posit_rgemm_workspace_size.restype = _c.c_size_t
 _lib.posit_device_error.argtypes = [_c.c_int]
@@ -156,6 +158,26 @@ def to_double_dev(u, out=None, stream=None):
     _check(_lib.posit_to_double_dev(u.data_ptr(), out.data_ptr(), u.numel(), stream.cuda_stream),
            "to_double")
     return out
+
+
+NOALLOC_SCRATCH_BYTES = 64 << 20
+POSIT_E_NOALLOC_LIMIT = -6
+
+
+def Rgemm_dev_noalloc(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream=None):
+    """Rgemm_dev for callers that cannot allocate device memory: the scratch is a
+    static 64 MiB device array inside the library (shared by all calls on a device; calls
+    that overlap on the GPU race).  Shapes needing more scratch raise PositError."""
+    import torch
+
+    for t in (A, B, C):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.element_size() == 4):
+            raise TypeError("Rgemm_dev_noalloc takes CUDA tensors of 4-byte elements")
+    if stream is None:
+        stream = torch.cuda.current_stream(C.device)
+    _check(_lib.posit_rgemm_dev_noalloc(_char(transa), _char(transb), m, n, k, int(alpha) & 0xFFFFFFFF,
+                                        A.data_ptr(), lda, B.data_ptr(), ldb, int(beta) & 0xFFFFFFFF,
+                                        C.data_ptr(), ldc, stream.cuda_stream), "Rgemm ")
 
 
 def device_error(clear=True):

@@ -241,6 +241,8 @@ const char *posit_strerror(int code)
         return "kernel error flag raised (bounded wait expired)";
     case POSIT_E_WORKSPACE:
         return "workspace too small or misaligned";
+    case POSIT_E_NOALLOC_LIMIT:
+        return "shape needs more scratch than the allocation-free entry point's static array";
     default:
         if (code > 0)
             return "illegal argument (BLAS info = parameter number)";
