@@ -61,7 +61,8 @@ int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alph
  * scratch is a static device array of POSIT_NOALLOC_SCRATCH_BYTES compiled into the
  * library, held by every GPU that loads the library until the process exits.  Shapes
  * whose posit_rgemm_workspace_size exceeds that size return POSIT_E_NOALLOC_LIMIT (e.g.
- * 2048^3 fits exactly; an 8192 x 8192 x 256 trailing update needs 34 MB and fits).
+ * 2048 x 2048 x 2032 fits, 2048^3 does not; an 8192 x 8192 x 256 trailing update needs
+ * 34 MB and fits).
  * The first call on a device looks up the array's address; make it before any stream
  * capture.  All calls share the array: calls that overlap on the GPU race. */
 #define POSIT_NOALLOC_SCRATCH_BYTES (64u << 20)

@@ -112,13 +112,14 @@ GemmPlan gemm_plan(int m, int n, int k)
     p.kt = (k + BK - 1) / BK;
     p.a_bytes = (size_t)p.mt * p.kt * BK * BM * sizeof(uint2);
     p.b_bytes = (size_t)p.nt * p.kt * BK * BN * sizeof(uint2);
+    p.flag_bytes = (size_t)(p.mt * BM + p.nt * BN);
     return p;
 }
 
 size_t gemm_workspace_bytes(int m, int n, int k)
 {
     GemmPlan p = gemm_plan(m, n, k);
-    return p.a_bytes + p.b_bytes;
+    return p.a_bytes + p.b_bytes + p.flag_bytes;
 }
 
 // ---------------------------------------------------------------------------
@@ -126,8 +127,11 @@ size_t gemm_workspace_bytes(int m, int n, int k)
 // ---------------------------------------------------------------------------
 // op(A) (m x k) -> Ad[mt][kt][l][i].  Rows/columns beyond the matrix hold 1.0 so that
 // padded lanes stay on the fast path; their results are never stored.
+// A NaR operand makes every output of its row NaR (p32_mul and p32_add propagate NaR,
+// kernel_entry.cl:385-390, 414-417); that is recorded in row_nar[] and the operand is
+// decoded as 1.0 so the row's arithmetic stays on the fast path.
 __global__ void decode_a_kernel(bool nota, int m, int k, const uint32_t *__restrict__ A, size_t lda,
-                                int KT, size_t total, uint2 *__restrict__ Ad)
+                                int KT, size_t total, uint2 *__restrict__ Ad, unsigned char *__restrict__ row_nar)
 {
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
@@ -141,13 +145,18 @@ __global__ void decode_a_kernel(bool nota, int m, int k, const uint32_t *__restr
         uint32_t u = P32_ONE;
         if (row < m && kk < k)
             u = nota ? A[(size_t)row + (size_t)kk * lda] : A[(size_t)kk + (size_t)row * lda];
-        Ad[idx] = pack_dp(decode(u));
+        if (u == P32_NAR) {
+            row_nar[row] = 1;
+            u = P32_ONE;
+        }
+        Ad[idx] = pack_dp(decode_gemm(u));
     }
 }
 
 // op(B) (k x n) -> Td[nt][kt][l][j], times alpha (exactly rounded) when `scale`.
 __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restrict__ B, size_t ldb,
-                                bool scale, uint32_t alpha, int KT, size_t total, uint2 *__restrict__ Td)
+                                bool scale, uint32_t alpha, int KT, size_t total, uint2 *__restrict__ Td,
+                                unsigned char *__restrict__ col_nar)
 {
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
@@ -164,7 +173,11 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
             if (scale)
                 u = pmul(alpha, u); // Rgemm.cpp:180 / 222: temp = alpha*b
         }
-        Td[idx] = pack_dp(decode(u));
+        if (u == P32_NAR) {
+            col_nar[col] = 1;
+            u = P32_ONE;
+        }
+        Td[idx] = pack_dp(decode_gemm(u));
     }
 }
 
@@ -176,40 +189,47 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
 __device__ __forceinline__ int own_off(int t, int q) { return (q >> 1) * 32 + 2 * t + (q & 1); }
 
 template <bool DOT>
-__global__ void __launch_bounds__(NTHREADS, 2)
+__global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     gemm_main_kernel(int m, int n, int k, int KT, uint32_t alpha, uint32_t beta,
                      const uint2 *__restrict__ Ad, const uint2 *__restrict__ Td, uint32_t *__restrict__ C,
-                     size_t ldc)
+                     size_t ldc, const unsigned char *__restrict__ row_nar,
+                     const unsigned char *__restrict__ col_nar)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint2 *As = reinterpret_cast<uint2 *>(smem_raw);
     uint2 *Ts = As + STAGES * BK * BM;
+    RegimeEntry *rtab = reinterpret_cast<RegimeEntry *>(Ts + STAGES * BK * BN);
+    const RegimeEntry *tbl = rtab - RT_MIN; // tbl[s] for RT_MIN <= s <= RT_MAX
     __shared__ __align__(8) uint64_t full[STAGES];
 
     const int tid = threadIdx.x;
-    const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+    const int tx = tid % 16, ty = tid / 16;
     const int mt = blockIdx.x, nt = blockIdx.y;
     const uint2 *Ablk = Ad + (size_t)mt * KT * BK * BM;
     const uint2 *Tblk = Td + (size_t)nt * KT * BK * BN;
-    constexpr uint32_t kTileBytes = BK * BM * sizeof(uint2);
-    static_assert(BM == BN, "one tile size for both operands");
+    constexpr uint32_t kATileBytes = BK * BM * sizeof(uint2);
+    constexpr uint32_t kBTileBytes = BK * BN * sizeof(uint2);
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s)
             mbar_init(&full[s], 1);
         mbar_fence_init();
     }
+    for (int i = tid; i < RT_N; i += NTHREADS)
+        rtab[i] = regime_entry(RT_MIN + i);
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < STAGES && s < KT; ++s) {
-            mbar_arrive_expect_tx(&full[s], 2 * kTileBytes);
-            bulk_g2s(As + s * BK * BM, Ablk + (size_t)s * BK * BM, kTileBytes, &full[s]);
-            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)s * BK * BN, kTileBytes, &full[s]);
+            mbar_arrive_expect_tx(&full[s], kATileBytes + kBTileBytes);
+            bulk_g2s(As + s * BK * BM, Ablk + (size_t)s * BK * BM, kATileBytes, &full[s]);
+            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)s * BK * BN, kBTileBytes, &full[s]);
         }
     }
 
-    // Accumulators: NN/NT start from beta*C, TN/TT from zero.
+    // Accumulators: NN/NT start from beta*C, TN/TT from zero.  A NaR start value is
+    // remembered in nar_bits (the output stays NaR whatever follows) and replaced by 1.0.
     dp32 acc[TM][TN];
+    uint32_t nar_bits = 0;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
 #pragma unroll
@@ -225,8 +245,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
                     else if (beta != P32_ONE)
                         u = pmul(beta, u);
                 }
+                if (u == P32_NAR) {
+                    nar_bits |= 1u << (i * TN + j);
+                    u = P32_ONE;
+                }
             }
-            acc[i][j] = decode(u);
+            acc[i][j] = decode_gemm(u);
         }
     }
 
@@ -241,31 +265,35 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         const uint2 *ts = Ts + s * BK * BN;
         const int lmax = min(BK, k - kt * BK);
         for (int l = 0; l < lmax; ++l) {
-            const uint4 a01 = *reinterpret_cast<const uint4 *>(as + l * BM + 2 * tx);
-            const uint4 a23 = *reinterpret_cast<const uint4 *>(as + l * BM + 32 + 2 * tx);
-            const uint4 t01 = *reinterpret_cast<const uint4 *>(ts + l * BN + 2 * ty);
-            const uint4 t23 = *reinterpret_cast<const uint4 *>(ts + l * BN + 32 + 2 * ty);
             dp32 a[TM], t[TN];
-            a[0] = unpack_dp(a01.x, a01.y);
-            a[1] = unpack_dp(a01.z, a01.w);
-            a[2] = unpack_dp(a23.x, a23.y);
-            a[3] = unpack_dp(a23.z, a23.w);
-            t[0] = unpack_dp(t01.x, t01.y);
-            t[1] = unpack_dp(t01.z, t01.w);
-            t[2] = unpack_dp(t23.x, t23.y);
-            t[3] = unpack_dp(t23.z, t23.w);
+#pragma unroll
+            for (int q = 0; q < TM / 2; ++q) {
+                const uint4 v = *reinterpret_cast<const uint4 *>(as + l * BM + 32 * q + 2 * tx);
+                a[2 * q] = unpack_dp(v.x, v.y);
+                a[2 * q + 1] = unpack_dp(v.z, v.w);
+            }
+#pragma unroll
+            for (int q = 0; q < TN / 2; ++q) {
+                const uint4 v = *reinterpret_cast<const uint4 *>(ts + l * BN + 32 * q + 2 * ty);
+                t[2 * q] = unpack_dp(v.x, v.y);
+                t[2 * q + 1] = unpack_dp(v.z, v.w);
+            }
             uint32_t fail = 0;
 #pragma unroll
             for (int i = 0; i < TM; ++i) {
 #pragma unroll
                 for (int j = 0; j < TN; ++j) {
                     dp32 p, r;
-                    bool ok = dmul_fast(t[j], a[i], p);
-                    ok = dadd_fast(acc[i][j], p, r) && ok;
-                    if (ok)
-                        acc[i][j] = r;
-                    else
-                        fail |= 1u << (i * TN + j);
+                    uint32_t bm, ba;
+                    dmul_fast(t[j], a[i], tbl, p, bm);
+                    dadd_fast(acc[i][j], p, tbl, r, ba);
+                    // branch-free commit: a failed step leaves the accumulator as it was,
+                    // and sets bit i*TN+j of `fail` (umulhi(2^30, 2^(idx+2)) = 2^idx)
+                    const uint32_t v = (bm | ba) & 0x40000000u;
+                    acc[i][j].s = v ? acc[i][j].s : r.s;
+                    acc[i][j].g = v ? acc[i][j].g : r.g;
+                    acc[i][j].x = v ? acc[i][j].x : r.x;
+                    fail += __umulhi(v, 4u << (i * TN + j));
                 }
             }
             if (fail) { // rare: redo the failed steps exactly, in the same order
@@ -283,9 +311,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             break;
         if (tid == 0 && kt + STAGES < KT) {
             const int nk = kt + STAGES;
-            mbar_arrive_expect_tx(&full[s], 2 * kTileBytes);
-            bulk_g2s(As + s * BK * BM, Ablk + (size_t)nk * BK * BM, kTileBytes, &full[s]);
-            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)nk * BK * BN, kTileBytes, &full[s]);
+            mbar_arrive_expect_tx(&full[s], kATileBytes + kBTileBytes);
+            bulk_g2s(As + s * BK * BM, Ablk + (size_t)nk * BK * BM, kATileBytes, &full[s]);
+            bulk_g2s(Ts + s * BK * BN, Tblk + (size_t)nk * BK * BN, kBTileBytes, &full[s]);
         }
     }
 
@@ -306,7 +334,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             const int row = mt * BM + own_off(tx, i), col = nt * BN + own_off(ty, j);
             if (row < m && col < n) {
                 uint32_t *cp = C + (size_t)row + (size_t)col * ldc;
-                uint32_t v = encode(acc[i][j]);
+                const bool nar = ((nar_bits >> (i * TN + j)) & 1u) || row_nar[row] || col_nar[col];
+                uint32_t v = nar ? P32_NAR : encode(acc[i][j]);
                 if (DOT) { // Rgemm.cpp:197-201
                     uint32_t at = pmul(alpha, v);
                     v = (beta == 0) ? at : padd(at, pmul(beta, *cp));
@@ -417,14 +446,19 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
     GemmPlan p = gemm_plan(m, n, k);
     uint2 *Ad = reinterpret_cast<uint2 *>(workspace);
     uint2 *Td = reinterpret_cast<uint2 *>(reinterpret_cast<unsigned char *>(workspace) + p.a_bytes);
+    unsigned char *row_nar = reinterpret_cast<unsigned char *>(workspace) + p.a_bytes + p.b_bytes;
+    unsigned char *col_nar = row_nar + (size_t)p.mt * BM;
     const bool dot = !nota; // TN / TT use the dot-then-combine order
     size_t na = p.a_bytes / sizeof(uint2), nb = p.b_bytes / sizeof(uint2);
-    decode_a_kernel<<<grid_for(na, 256), 256, 0, stream>>>(nota, m, k, A, (size_t)lda, p.kt, na, Ad);
+    cudaError_t e = cudaMemsetAsync(row_nar, 0, p.flag_bytes, stream);
+    if (e != cudaSuccess)
+        return e;
+    decode_a_kernel<<<grid_for(na, 256), 256, 0, stream>>>(nota, m, k, A, (size_t)lda, p.kt, na, Ad, row_nar);
     decode_b_kernel<<<grid_for(nb, 256), 256, 0, stream>>>(notb, k, n, B, (size_t)ldb, !dot, alpha, p.kt, nb,
-                                                           Td);
-    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2);
+                                                           Td, col_nar);
+    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2) + (size_t)RT_N * sizeof(RegimeEntry);
     dim3 grid(p.mt, p.nt);
-    cudaError_t e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem)
                         : cudaFuncSetAttribute(gemm_main_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
@@ -433,9 +467,11 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
     const bool prof = g_prof_on;
     cudaEvent_t e0 = prof ? prof_mark(stream) : nullptr;
     if (dot)
-        gemm_main_kernel<true><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
+        gemm_main_kernel<true><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc,
+                                                                 row_nar, col_nar);
     else
-        gemm_main_kernel<false><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc);
+        gemm_main_kernel<false><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
+                                                                  (size_t)ldc, row_nar, col_nar);
     if (prof) {
         cudaEvent_t e1 = prof_mark(stream);
         std::lock_guard<std::mutex> lk(g_prof_mu);

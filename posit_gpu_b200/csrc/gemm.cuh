@@ -6,14 +6,17 @@
 
 namespace pg {
 
-// Output tile of one CTA and the k-depth of one staged tile.
-constexpr int BM = 64;
-constexpr int BN = 64;
-constexpr int BK = 16;
+// Output tile of one CTA and the k-depth of one staged tile.  A thread owns TM x TN
+// outputs; 16 x 16 threads; rows and columns are owned in pairs 32 apart (own_off).
 constexpr int TM = 4; // rows per thread
-constexpr int TN = 4; // columns per thread
-constexpr int NTHREADS = (BM / TM) * (BN / TN);
+constexpr int TN = 2; // columns per thread
+constexpr int BM = 16 * TM;
+constexpr int BN = 16 * TN;
+constexpr int BK = 16;
+constexpr int NTHREADS = 256;
 constexpr int STAGES = 3;
+constexpr int MIN_CTAS_PER_SM = 3;
+static_assert(TM % 2 == 0 && TN % 2 == 0, "operands are loaded in pairs");
 
 // Error flags a kernel can raise (read back with posit_get_device_error).
 constexpr int DEV_ERR_WAIT_TIMEOUT = 1;
@@ -21,7 +24,7 @@ constexpr int DEV_ERR_WAIT_TIMEOUT = 1;
 struct GemmPlan {
     int m, n, k;
     int mt, nt, kt; // tile counts
-    size_t a_bytes, b_bytes;
+    size_t a_bytes, b_bytes, flag_bytes;
 };
 
 GemmPlan gemm_plan(int m, int n, int k);

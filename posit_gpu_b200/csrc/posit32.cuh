@@ -345,17 +345,43 @@ PG_HD uint32_t pabs(uint32_t a) { return ((int32_t)a < 0) ? 0u - a : a; }
 // ----------------------------------------------------------------------------
 // Decoded-domain operations for the GEMM inner loop
 // ----------------------------------------------------------------------------
+//
+// The inner loop is integer code bound by the ALU pipe, so it is written to put as
+// much of its work as possible on the (otherwise idle) integer multiply-add pipe:
+//   * every quantity that depends only on a result's scale (regime run length, the
+//     multipliers that shift by it, whether the fast path is exact there) comes from a
+//     table indexed by that scale (one 16-byte shared-memory load);
+//   * right shifts by n are multiplies by 2^(32-n) keeping the high word, and a 64-bit
+//     funnel shift is two multiply-adds;
+//   * round-to-nearest-even at bit 32 is one 64-bit add of 0x7FFFFFFF + lsb.
+// In the fast path the smaller addend is shifted by at most 30 bits inside a 64-bit
+// frame, so no bit of it is lost and the sum is exact: the reference's truncating
+// alignment (kernel_entry.cl:154, 292-298) can only matter beyond that, where the step
+// is handed to the exact path instead.
 
-// Round a value whose significand T-window has already been formed: `thi` holds the
-// hidden bit and the kept fraction bits (hidden at bit 28-run), `tlo` the guard bit
-// (bit 31) and the sticky bits (30..0).  Round to nearest even on the last kept bit.
-PG_HD void round_window(uint32_t thi, uint32_t tlo, int32_t s, uint32_t run, dp32 &r)
+// Multiply-high and 64-bit multiply-add (single integer multiply-add instructions).
+PG_HD uint32_t umulhi(uint32_t a, uint32_t b)
 {
-    uint32_t up = (tlo | (thi & 1u)) > 0x80000000u ? 1u : 0u;
-    uint32_t g = shl32(thi + up, run + 2); // hidden back at bit 30, or 31 on carry-out
-    uint32_t ov = g >> 31;
-    r.s = s + (int32_t)ov;
-    r.g = g >> ov;
+#if defined(__CUDA_ARCH__)
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+// Round to nearest even at bit 32 of (thi:tlo), returning the rounded high word:
+// thi + carry-out of (tlo | lsb) + 0x7FFFFFFF.  On the GPU this is one 32x32+64-bit
+// multiply-add (integer multiply-add pipe) instead of an add-with-carry pair.
+PG_HD uint32_t round_hi(uint32_t thi, uint32_t tlo)
+{
+    uint32_t v = tlo | (thi & 1u);
+#if defined(__CUDA_ARCH__)
+    uint64_t acc = ((uint64_t)thi << 32) | 0x7FFFFFFFu, r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(v), "r"(1u), "l"(acc));
+    return (uint32_t)(r >> 32);
+#else
+    return thi + (uint32_t)(((uint64_t)v + 0x7FFFFFFFu) >> 32);
+#endif
 }
 
 PG_HD uint32_t regime_run(int32_t s)
@@ -366,72 +392,125 @@ PG_HD uint32_t regime_run(int32_t s)
 
 PG_HD bool in_fast_range(int32_t s) { return (uint32_t)(s - FAST_LO) <= (uint32_t)(FAST_HI - FAST_LO); }
 
-// t*a rounded to posit32, both operands decoded.  Returns false (result unusable) if
-// the result's regime is longer than 27 bits, or an operand is zero or NaR.
-PG_HD bool dmul_fast(const dp32 &t, const dp32 &a, dp32 &r)
+// Decoded zero inside the GEMM kernels.  Any product with a zero operand then has a
+// scale <= ZERO_SCALE + 121 < ZERO_REGION, below every nonzero product (>= -241) and
+// every nonzero sum (>= -270), and its significand is 0.
+constexpr int32_t GEMM_ZERO_SCALE = -512;
+constexpr int32_t ZERO_REGION = -300;
+
+// Regime table: one entry per result scale s in [RT_MIN, RT_MAX].
+struct alignas(16) RegimeEntry {
+    uint32_t r0;  // 2^(32-run): umulhi by it shifts right by run
+    uint32_t nr1; // -(2^(31-run)); r0 + carry*nr1 = 2^(32-run-carry).  Bit 30 set
+                  // means "a zero significand here is a failure" (clear in the zero region)
+    uint32_t g;   // 2^(run+2): moves the kept bits back to a hidden bit at 30
+    uint32_t w;   // 2^(29-run) (window multiplier for a hidden bit at 63), bit 30 = fail
+};
+constexpr int32_t RT_MIN = 2 * GEMM_ZERO_SCALE - 40;
+constexpr int32_t RT_MAX = 248;
+constexpr int32_t RT_N = RT_MAX - RT_MIN + 1;
+
+PG_HD RegimeEntry regime_entry(int32_t s)
 {
-    uint64_t p = (uint64_t)t.g * a.g;
-    uint32_t hi = (uint32_t)(p >> 32), lo = (uint32_t)p;
-    uint32_t carry = hi >> 29; // hidden bit at 61 instead of 60
-    int32_t s = t.s + a.s + (int32_t)carry;
-    uint32_t run = regime_run(s);
-    uint32_t sh = run + carry; // the reference's (frac >> carry) >> run
-    uint32_t tlo = shr64_lo(lo, hi, sh);
-    uint32_t thi = shr32(hi, sh);
-    round_window(thi, tlo, s, run, r);
-    r.x = t.x ^ a.x;
-    return in_fast_range(s);
+    RegimeEntry e;
+    bool zero_region = s < ZERO_REGION;
+    bool fast = in_fast_range(s);
+    uint32_t run = (fast && !zero_region) ? regime_run(s) : 27u;
+    e.r0 = 1u << (32 - run);
+    e.nr1 = zero_region ? 0u : 0u - (1u << (31 - run));
+    e.g = 1u << (run + 2);
+    e.w = (1u << (29 - run)) | ((fast || zero_region) ? 0u : 0x40000000u);
+    return e;
 }
 
-// c + p rounded to posit32, both decoded.  Returns false if the exact path is needed:
-// result regime longer than 27 bits, NaR, or an exactly zero sum.
-PG_HD bool dadd_fast(const dp32 &c, const dp32 &p, dp32 &r)
+// t*a rounded to posit32 (kernel_entry.cl:399-538), both operands decoded and nonzero
+// or decoded zeros.  `bad` gets bit 30 set when the result must come from the exact path
+// (regime longer than 27 bits, or rounding carried out of the significand).
+PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
 {
-    int32_t d = c.s - p.s;
-    bool sw = d < 0;
+    uint64_t P = (uint64_t)t.g * a.g; // hidden bit at 60, or 61 ("carry")
+    uint32_t hi = (uint32_t)(P >> 32), lo = (uint32_t)P;
+    uint32_t carry = umulhi(hi, 8u);
+    int32_t s = t.s + a.s + (int32_t)carry;
+    const RegimeEntry e = tbl[s];
+    uint32_t W = e.r0 + carry * e.nr1; // 2^(32 - run - carry)
+    // T = P >> (run + carry): kept bits in thi (hidden at 28-run), guard+sticky in tlo
+    uint32_t thi = umulhi(hi, W);
+    uint32_t tlo = hi * W + umulhi(lo, W);
+    r.g = round_hi(thi, tlo) * e.g;
+    r.s = s;
+    r.x = t.x ^ a.x;
+    bad = e.w | (~r.g & e.nr1);
+}
+
+// c + p rounded to posit32 (kernel_entry.cl:370-397), both decoded.  Fails (bit 30 of
+// `bad`) for a result regime longer than 27 bits, an exactly cancelling sum of nonzero
+// values, or a rounding carry-out.
+// An addend more than 30 binades below the other contributes nothing here (Q = 0), and
+// that is also the reference's result: in its 64-bit frame (hidden bit at 62) such an
+// addend is below 2^32, i.e. entirely under the guard bit of the larger operand, whose
+// bits below its last kept bit are zero.  A sum then rounds back to the larger operand;
+// a difference A - e (0 < e < 2^32) borrows ones through every bit up to A's last kept
+// bit, so guard and sticky are set and it rounds up to A again -- including when A is a
+// power of two, since the spacing below A is at least 2^(33+run) frame units.
+PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
+{
+    // order by magnitude: scale, then significand (so the difference is never negative).
+    // Bitwise, not short-circuit, operators: the latter compile to branches, which both
+    // cost issue slots and stop the scheduler from interleaving independent steps.
+    bool sw = (c.s < p.s) | ((c.s == p.s) & (c.g < p.g));
     int32_t bs = sw ? p.s : c.s;
     uint32_t bg = sw ? p.g : c.g;
-    uint32_t bx = sw ? p.x : c.x;
     uint32_t sg = sw ? c.g : p.g;
-    uint32_t ad = (uint32_t)(sw ? -d : d);
-    ad = ad > 63u ? 63u : ad;
-    // the smaller operand in the 64-bit frame (hidden at 62), truncated at bit 0
-    uint64_t B = ((uint64_t)sg << 32) >> ad;
-    uint64_t A = (uint64_t)bg << 32;
-    uint64_t S = (c.x ^ p.x) ? A - B : A + B;
-    // equal scales and opposite signs may leave a negative difference
-    uint32_t neg = (uint32_t)(S >> 63) & (c.x ^ p.x);
-    S = neg ? 0ull - S : S;
-    uint32_t shi = (uint32_t)(S >> 32);
-    uint32_t lz = clz32(shi); // S.hi == 0 only when S == 0
-    // normalise to the hidden bit at 63 (bits shifted in are zero); lz <= 32
-    uint64_t N = S << lz;
-    uint32_t nhi = (uint32_t)(N >> 32), nlo = (uint32_t)N;
-    int32_t s = bs + 1 - (int32_t)lz;
-    uint32_t run = regime_run(s);
-    uint32_t sh = run + 3;
-    uint32_t tlo = shr64_lo(nlo, nhi, sh);
-    uint32_t thi = shr32(nhi, sh);
-    round_window(thi, tlo, s, run, r);
-    r.x = bx ^ neg;
-    return in_fast_range(s) && shi != 0;
+    uint32_t bx = sw ? p.x : c.x;
+    int32_t d = c.s - p.s;
+    uint32_t ad = (uint32_t)(d < 0 ? -d : d);
+    uint32_t Q = shr32(0x40000000u, ad); // 2^(30-ad); 0 beyond 30
+    int32_t M = (c.x ^ p.x) ? -(int32_t)Q : (int32_t)Q;
+    // frame: the larger significand's hidden bit at 60; exact for ad <= 30
+    uint64_t S = (uint64_t)(((int64_t)bg << 30) + (int64_t)(int32_t)sg * (int64_t)M);
+    uint32_t shi = (uint32_t)(S >> 32), slo = (uint32_t)S;
+    uint32_t lz = clz32(shi);         // S.hi == 0 only when S == 0
+    int32_t s = bs + 3 - (int32_t)lz; // result scale
+    const RegimeEntry e = tbl[s];
+    uint32_t p2 = shl32(1u, lz);
+    uint32_t nhi = shi * p2 + umulhi(slo, p2); // N = S << lz: hidden bit at 63
+    uint32_t nlo = slo * p2;
+    uint32_t thi = umulhi(nhi, e.w); // T = N >> (run + 3)
+    uint32_t tlo = nhi * e.w + umulhi(nlo, e.w);
+    r.g = round_hi(thi, tlo) * e.g;
+    r.s = s;
+    r.x = bx;
+    bad = e.w | (~r.g & e.nr1);
 }
 
-// Exact decoded operations (through patterns): the slow path.
-PG_HD_NOINLINE dp32 dmul_exact(dp32 t, dp32 a) { return decode(pmul(encode(t), encode(a))); }
-PG_HD_NOINLINE dp32 dadd_exact(dp32 c, dp32 p) { return decode(padd(encode(c), encode(p))); }
+// Exact decoded operations (through patterns): the slow path.  Decoded zeros of the
+// GEMM kernels (significand 0) encode to the zero pattern.
 PG_HD_NOINLINE dp32 dmac_exact(dp32 c, dp32 t, dp32 a)
 {
-    return decode(padd(encode(c), pmul(encode(t), encode(a))));
+    dp32 r = decode(padd(encode(c), pmul(encode(t), encode(a))));
+    if (r.g == 0)
+        r.s = GEMM_ZERO_SCALE;
+    return r;
 }
 
-// c + t*a with both roundings; never fails.
-PG_HD dp32 dmac(const dp32 &c, const dp32 &t, const dp32 &a)
+// Decode for the GEMM kernels: zero gets GEMM_ZERO_SCALE; NaR is the caller's business.
+PG_HD dp32 decode_gemm(uint32_t u)
+{
+    dp32 d = decode(u);
+    if (u == 0)
+        d.s = GEMM_ZERO_SCALE;
+    return d;
+}
+
+// c + t*a with both roundings; never fails.  tbl points at the entry for scale 0.
+PG_HD dp32 dmac(const dp32 &c, const dp32 &t, const dp32 &a, const RegimeEntry *tbl)
 {
     dp32 p, r;
-    bool ok = dmul_fast(t, a, p);
-    ok = dadd_fast(c, p, r) && ok;
-    if (!ok)
+    uint32_t bm, ba;
+    dmul_fast(t, a, tbl, p, bm);
+    dadd_fast(c, p, tbl, r, ba);
+    if ((bm | ba) & 0x40000000u)
         r = dmac_exact(c, t, a);
     return r;
 }

@@ -80,4 +80,8 @@ def test_strerror_and_workspace_size():
     assert b"argument" in pg._lib.posit_strerror(8)
     assert pg.workspace_size("N", "N", 0, 5, 5) == 0
     ws = pg.workspace_size("N", "T", 100, 70, 33)
-    assert ws == (2 * 64 * 48 + 2 * 64 * 48) * 8  # 2 m-tiles, 2 n-tiles, 3 k-tiles of 16
+    # decoded operands: 8 bytes per element of op(A) and op(B), padded to whole tiles,
+    # plus one NaR flag byte per padded row and column
+    assert ws >= 8 * (100 + 70) * 33 + 100 + 70
+    assert ws < 8 * (100 + 70 + 2 * 64) * (33 + 16) + 1024
+    assert pg.workspace_size("N", "T", 100, 70, 66) > ws
