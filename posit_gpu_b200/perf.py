@@ -14,14 +14,15 @@ SM_MAX_MHZ = 1965.0
 
 # Warp instructions issued by gemm_main_kernel per posit multiply-add:
 # smsp__inst_executed.sum / (m*n*k) for one NN launch at m = n = k = 4096
-# (163,938,025,447 / 68,719,476,736).  Practically all of them are integer ALU / FMA-pipe
-# instructions (ALU pipe 92.3 % and FMA pipe 15.1 % of peak in the same capture).
-INT_PIPE_WARP_INST_PER_MAD = 2.3856
+# (119,155,165,229 / 68,719,476,736).  Practically all of them are integer ALU or
+# integer multiply-add (FMA-pipe) instructions (ALU pipe 61.1 %, FMA pipes 35.0 % busy in
+# the same capture; table and operand loads are 0.07 per MAD).
+INT_PIPE_WARP_INST_PER_MAD = 1.7339
 INST_SOURCE = ("ncu --set full, gemm_main_kernel<false>, NN 4096^3 U[-1,1] "
                "(profiles/gemm_main_kernel_nn_4096.md)")
 # DRAM bytes (read + write) per posit multiply-add of the same launch:
-# (3,917,192,000 + 173,531,392) / 68,719,476,736.
-MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.05953
+# (7,432,703,000 + 73,915,648) / 68,719,476,736.
+MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1092
 
 
 def issue_peak_warp_inst_per_s(sm_mhz):
