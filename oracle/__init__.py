@@ -101,6 +101,22 @@ def _load_ref():
     return lib
 
 
+def load_ref_dropin():
+    """The reference's own Rgetrf_opencl / Rpotrf_opencl linked against the B200 RgemmG
+    (oracle/_ref/libposit_ref_dropin.so), or None where it was not built.  Loading it
+    loads the CUDA library, so only GPU tests call this."""
+    path = os.path.join(HERE, "_ref", "libposit_ref_dropin.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    i32 = _c.c_int
+    lib.refd_rgetrf_opencl.argtypes = [i32, i32, _U32P, i32, _I32P, i32]
+    lib.refd_rgetrf_opencl.restype = i32
+    lib.refd_rpotrf_opencl.argtypes = [_c.c_char, i32, _U32P, i32, i32]
+    lib.refd_rpotrf_opencl.restype = i32
+    return lib
+
+
 orc = _load_orc()
 ref = _load_ref()
 
