@@ -26,6 +26,7 @@ extern "C" {
 #define POSIT_E_DEVICE_FAULT (-4) /* a kernel raised its error flag (bounded wait expired) */
 #define POSIT_E_WORKSPACE (-5)    /* caller-provided workspace too small */
 #define POSIT_E_NOALLOC_LIMIT (-6) /* shape needs more scratch than posit_rgemm_dev_noalloc has */
+#define POSIT_E_UNSUPPORTED (-7)   /* a variant this library does not implement on the device */
 
 /* Replaces initOpenCL (libRpack/def.h:63, libRpack/Rgemm_opencl.cpp:59-70): selects
  * the current CUDA device, creates its context and warms the kernels.  Optional: every
@@ -72,6 +73,33 @@ int posit_rgemm_dev_noalloc(char transa, char transb, int m, int n, int k, uint3
 
 /* Bytes of device workspace posit_rgemm_dev needs for this shape (0 when none). */
 size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k);
+
+/* ---- Device-resident factorizations and solves ------------------------------------
+ * Bit-identical to the reference's CPU Rgetrf / Rgetrs / Rpotrf / Rpotrs (at any block
+ * size: LU and lower Cholesky in the reference's operation order do not depend on it,
+ * for inputs without NaR).  Return value: 0, the number of an illegal argument (as the
+ * reference passes to Mxerbla: 1, 2, 4, ... ), or a negative POSIT_E_* code.  The
+ * numerical result goes to *info exactly as in the reference (first zero pivot / first
+ * non-positive leading minor, 1-based; 0 on success).  nb <= 0 selects 256.
+ *
+ * _dev forms: device pointers (ipiv and info included: *info is written on the device,
+ * asynchronously on `stream`); workspace is stream-ordered.  Host forms: host pointers,
+ * synchronous.  Only trans = 'N' (Rgetrs) and uplo = 'L' (Rpotrf/Rpotrs) run on the
+ * device; the others return POSIT_E_UNSUPPORTED. */
+
+/* Rgetrf (libRpack/Rgetrf.cpp:32-137; mplapack_posit.h:104), Rgetrf_opencl (mplapack_posit.h:105) */
+int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream);
+int posit_rgetrf(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info);
+/* Rgetrs (libRpack/Rgetrs.cpp:32-118; mplapack_posit.h:102) */
+int posit_rgetrs_dev(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B,
+                     int ldb, void *stream);
+int posit_rgetrs(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb);
+/* Rpotrf (libRpack/Rpotrf.cpp:32-154; mplapack_posit.h:94), Rpotrf_opencl (mplapack_posit.h:99) */
+int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, void *stream);
+int posit_rpotrf(char uplo, int n, uint32_t *A, int lda, int nb, int *info);
+/* Rpotrs (libRpack/Rpotrs.cpp:32-110; mplapack_posit.h:97) */
+int posit_rpotrs_dev(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, void *stream);
+int posit_rpotrs(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb);
 
 /* Element-wise conversions on device buffers, asynchronous on `stream`.
  * Replace the SoftPosit class conversions the reference drivers use to build their

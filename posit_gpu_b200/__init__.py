@@ -52,6 +52,18 @@ _lib.posit_from_double_dev.argtypes = [_VP, _VP, _c.c_size_t, _VP]
 _lib.posit_from_double_dev.restype = _c.c_int
 _lib.posit_to_double_dev.argtypes = [_VP, _VP, _c.c_size_t, _VP]
 _lib.posit_to_double_dev.restype = _c.c_int
+_I = _c.c_int
+_lib.posit_rgetrf_dev.argtypes = [_I, _I, _VP, _I, _VP, _I, _VP, _VP]
+_lib.posit_rgetrf.argtypes = [_I, _I, _VP, _I, _VP, _I, _c.POINTER(_I)]
+_lib.posit_rgetrs_dev.argtypes = [_c.c_char, _I, _I, _VP, _I, _VP, _VP, _I, _VP]
+_lib.posit_rgetrs.argtypes = [_c.c_char, _I, _I, _VP, _I, _VP, _VP, _I]
+_lib.posit_rpotrf_dev.argtypes = [_c.c_char, _I, _VP, _I, _I, _VP, _VP]
+_lib.posit_rpotrf.argtypes = [_c.c_char, _I, _VP, _I, _I, _c.POINTER(_I)]
+_lib.posit_rpotrs_dev.argtypes = [_c.c_char, _I, _I, _VP, _I, _VP, _I, _VP]
+_lib.posit_rpotrs.argtypes = [_c.c_char, _I, _I, _VP, _I, _VP, _I]
+for _f in ("posit_rgetrf_dev", "posit_rgetrf", "posit_rgetrs_dev", "posit_rgetrs", "posit_rpotrf_dev",
+           "posit_rpotrf", "posit_rpotrs_dev", "posit_rpotrs"):
+    getattr(_lib, _f).restype = _I
 _lib.posit_strerror.argtypes = [_c.c_int]
 _lib.posit_strerror.restype = _c.c_char_p
 
@@ -158,6 +170,69 @@ def to_double_dev(u, out=None, stream=None):
     _check(_lib.posit_to_double_dev(u.data_ptr(), out.data_ptr(), u.numel(), stream.cuda_stream),
            "to_double")
     return out
+
+
+# ---------------------------------------------------------------------------
+# LAPACK (libRpack/mplapack_posit.h:94-108): LU and Cholesky, bit-identical to the CPU
+# routines.  Host forms take numpy buffers (4-byte elements; ipiv int32) and return the
+# reference's `info`; _dev forms take torch CUDA tensors and leave info on the device.
+# ---------------------------------------------------------------------------
+def _host_i32(x):
+    if not (isinstance(x, np.ndarray) and x.dtype == np.int32):
+        raise TypeError("ipiv must be a numpy int32 array")
+    return x.ctypes.data
+
+
+def Rgetrf(m, n, A, lda, ipiv, nb=0):
+    """LU with partial pivoting in place (Rgetrf.cpp:32-137); ipiv 1-based. Returns info."""
+    info = _I(0)
+    _check(_lib.posit_rgetrf(m, n, _host_ptr(A), lda, _host_i32(ipiv), nb, _c.byref(info)), "Rgetrf")
+    return info.value
+
+
+def Rgetrs(trans, n, nrhs, A, lda, ipiv, B, ldb):
+    """Solve with an Rgetrf factorization (Rgetrs.cpp:32-118), B overwritten."""
+    _check(_lib.posit_rgetrs(_char(trans), n, nrhs, _host_ptr(A), lda, _host_i32(ipiv), _host_ptr(B), ldb),
+           "Rgetrs")
+
+
+def Rpotrf(uplo, n, A, lda, nb=0):
+    """Cholesky in place (Rpotrf.cpp:32-154). Returns info."""
+    info = _I(0)
+    _check(_lib.posit_rpotrf(_char(uplo), n, _host_ptr(A), lda, nb, _c.byref(info)), "Rpotrf")
+    return info.value
+
+
+def Rpotrs(uplo, n, nrhs, A, lda, B, ldb):
+    """Solve with an Rpotrf factor (Rpotrs.cpp:32-110), B overwritten."""
+    _check(_lib.posit_rpotrs(_char(uplo), n, nrhs, _host_ptr(A), lda, _host_ptr(B), ldb), "Rpotrs")
+
+
+def _stream_of(t, stream):
+    import torch
+    return (stream or torch.cuda.current_stream(t.device)).cuda_stream
+
+
+def Rgetrf_dev(m, n, A, lda, ipiv, info, nb=0, stream=None):
+    """Device LU: A (4-byte CUDA tensor), ipiv (int32 CUDA tensor, >= min(m,n)), info
+    (int32 CUDA tensor, 1 element, written on the device).  Asynchronous."""
+    _check(_lib.posit_rgetrf_dev(m, n, A.data_ptr(), lda, ipiv.data_ptr(), nb, info.data_ptr(),
+                                 _stream_of(A, stream)), "Rgetrf")
+
+
+def Rgetrs_dev(trans, n, nrhs, A, lda, ipiv, B, ldb, stream=None):
+    _check(_lib.posit_rgetrs_dev(_char(trans), n, nrhs, A.data_ptr(), lda, ipiv.data_ptr(), B.data_ptr(), ldb,
+                                 _stream_of(A, stream)), "Rgetrs")
+
+
+def Rpotrf_dev(uplo, n, A, lda, info, nb=0, stream=None):
+    _check(_lib.posit_rpotrf_dev(_char(uplo), n, A.data_ptr(), lda, nb, info.data_ptr(), _stream_of(A, stream)),
+           "Rpotrf")
+
+
+def Rpotrs_dev(uplo, n, nrhs, A, lda, B, ldb, stream=None):
+    _check(_lib.posit_rpotrs_dev(_char(uplo), n, nrhs, A.data_ptr(), lda, B.data_ptr(), ldb,
+                                 _stream_of(A, stream)), "Rpotrs")
 
 
 NOALLOC_SCRATCH_BYTES = 64 << 20

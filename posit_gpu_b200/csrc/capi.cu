@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI declared in include/posit_gpu.h.
 #include "../../include/posit_gpu.h"
 #include "gemm.cuh"
+#include "lapack.cuh"
 #include "posit32.cuh"
 
 #include <atomic>
@@ -197,6 +198,273 @@ int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, c
     return rc;
 }
 
+// ---- factorizations -------------------------------------------------------------
+static int pick_nb(int nb) { return nb > 0 ? nb : 256; }
+static cudaStream_t as_stream(void *stream) { return stream ? (cudaStream_t)stream : cudaStreamPerThread; }
+
+int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream)
+{
+    if (m < 0)
+        return 1; // Rgetrf.cpp:60-66
+    if (n < 0)
+        return 2;
+    if (lda < imax(1, m))
+        return 4;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = as_stream(stream);
+    PG_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
+    if (m == 0 || n == 0)
+        return 0;
+    nb = pick_nb(nb);
+    void *ws = nullptr;
+    PG_TRY(cudaMallocAsync(&ws, pg::rgetrf_workspace_bytes(m, n, nb), st));
+    cudaError_t e = pg::rgetrf_launch(m, n, A, lda, ipiv, nb, info, ws, st);
+    cudaFreeAsync(ws, st);
+    return e == cudaSuccess ? 0 : cuda_fail(e);
+}
+
+int posit_rgetrs_dev(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B,
+                     int ldb, void *stream)
+{
+    bool notr = same(trans, 'N');
+    if (!notr && !same(trans, 'T') && !same(trans, 'C'))
+        return 1; // Rgetrs.cpp:60-71
+    if (n < 0)
+        return 2;
+    if (nrhs < 0)
+        return 3;
+    if (lda < imax(1, n))
+        return 5;
+    if (ldb < imax(1, n))
+        return 8;
+    if (!notr)
+        return POSIT_E_UNSUPPORTED;
+    int r = ensure_init();
+    if (r)
+        return r;
+    if (n == 0 || nrhs == 0)
+        return 0;
+    PG_TRY(pg::rgetrs_launch(n, nrhs, A, lda, ipiv, B, ldb, as_stream(stream)));
+    return 0;
+}
+
+int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, void *stream)
+{
+    bool upper = same(uplo, 'U');
+    if (!upper && !same(uplo, 'L'))
+        return 1; // Rpotrf.cpp:64-72
+    if (n < 0)
+        return 2;
+    if (lda < imax(1, n))
+        return 4;
+    if (upper)
+        return POSIT_E_UNSUPPORTED;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = as_stream(stream);
+    PG_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
+    if (n == 0)
+        return 0;
+    nb = pick_nb(nb);
+    void *ws = nullptr;
+    PG_TRY(cudaMallocAsync(&ws, pg::rpotrf_workspace_bytes(n, nb), st));
+    cudaError_t e = pg::rpotrf_lower_launch(n, A, lda, nb, info, ws, st);
+    cudaFreeAsync(ws, st);
+    return e == cudaSuccess ? 0 : cuda_fail(e);
+}
+
+int posit_rpotrs_dev(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, void *stream)
+{
+    bool upper = same(uplo, 'U');
+    if (!upper && !same(uplo, 'L'))
+        return 1; // Rpotrs.cpp:60-71
+    if (n < 0)
+        return 2;
+    if (nrhs < 0)
+        return 3;
+    if (lda < imax(1, n))
+        return 5;
+    if (ldb < imax(1, n))
+        return 7;
+    if (upper)
+        return POSIT_E_UNSUPPORTED;
+    int r = ensure_init();
+    if (r)
+        return r;
+    if (n == 0 || nrhs == 0)
+        return 0;
+    PG_TRY(pg::rpotrs_lower_launch(n, nrhs, A, lda, B, ldb, as_stream(stream)));
+    return 0;
+}
+
+// Host forms: copy the referenced parts to the device, run, copy back, synchronise.
+static int finish(cudaStream_t st, int rc)
+{
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == 0 && e != cudaSuccess)
+        rc = cuda_fail(e);
+    if (rc == 0 && pg::read_device_error(true) != 0)
+        rc = POSIT_E_DEVICE_FAULT;
+    return rc;
+}
+
+int posit_rgetrf(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info)
+{
+    if (m < 0)
+        return 1;
+    if (n < 0)
+        return 2;
+    if (lda < imax(1, m))
+        return 4;
+    *info = 0;
+    if (m == 0 || n == 0)
+        return 0;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = cudaStreamPerThread;
+    uint32_t *dA = nullptr;
+    int *dp = nullptr;
+    const int mn = m < n ? m : n;
+    PG_TRY(cudaMallocAsync((void **)&dA, (size_t)m * n * 4, st));
+    PG_TRY(cudaMallocAsync((void **)&dp, ((size_t)mn + 1) * sizeof(int), st));
+    PG_TRY(cudaMemcpy2DAsync(dA, (size_t)m * 4, A, (size_t)lda * 4, (size_t)m * 4, n, cudaMemcpyHostToDevice, st));
+    int rc = posit_rgetrf_dev(m, n, dA, m, dp + 1, nb, dp, st);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(A, (size_t)lda * 4, dA, (size_t)m * 4, (size_t)m * 4, n,
+                                          cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ipiv, dp + 1, (size_t)mn * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(info, dp, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(e);
+    }
+    cudaFreeAsync(dA, st);
+    cudaFreeAsync(dp, st);
+    return finish(st, rc);
+}
+
+int posit_rgetrs(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb)
+{
+    bool notr = same(trans, 'N');
+    if (!notr && !same(trans, 'T') && !same(trans, 'C'))
+        return 1;
+    if (n < 0)
+        return 2;
+    if (nrhs < 0)
+        return 3;
+    if (lda < imax(1, n))
+        return 5;
+    if (ldb < imax(1, n))
+        return 8;
+    if (!notr)
+        return POSIT_E_UNSUPPORTED;
+    if (n == 0 || nrhs == 0)
+        return 0;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = cudaStreamPerThread;
+    uint32_t *dA = nullptr, *dB = nullptr;
+    int *dp = nullptr;
+    PG_TRY(cudaMallocAsync((void **)&dA, (size_t)n * n * 4, st));
+    PG_TRY(cudaMallocAsync((void **)&dB, (size_t)n * nrhs * 4, st));
+    PG_TRY(cudaMallocAsync((void **)&dp, (size_t)n * sizeof(int), st));
+    PG_TRY(cudaMemcpy2DAsync(dA, (size_t)n * 4, A, (size_t)lda * 4, (size_t)n * 4, n, cudaMemcpyHostToDevice, st));
+    PG_TRY(cudaMemcpy2DAsync(dB, (size_t)n * 4, B, (size_t)ldb * 4, (size_t)n * 4, nrhs, cudaMemcpyHostToDevice, st));
+    PG_TRY(cudaMemcpyAsync(dp, ipiv, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
+    int rc = posit_rgetrs_dev(trans, n, nrhs, dA, n, dp, dB, n, st);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(B, (size_t)ldb * 4, dB, (size_t)n * 4, (size_t)n * 4, nrhs,
+                                          cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(e);
+    }
+    cudaFreeAsync(dA, st);
+    cudaFreeAsync(dB, st);
+    cudaFreeAsync(dp, st);
+    return finish(st, rc);
+}
+
+int posit_rpotrf(char uplo, int n, uint32_t *A, int lda, int nb, int *info)
+{
+    bool upper = same(uplo, 'U');
+    if (!upper && !same(uplo, 'L'))
+        return 1;
+    if (n < 0)
+        return 2;
+    if (lda < imax(1, n))
+        return 4;
+    if (upper)
+        return POSIT_E_UNSUPPORTED;
+    *info = 0;
+    if (n == 0)
+        return 0;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = cudaStreamPerThread;
+    uint32_t *dA = nullptr;
+    int *di = nullptr;
+    PG_TRY(cudaMallocAsync((void **)&dA, (size_t)n * n * 4, st));
+    PG_TRY(cudaMallocAsync((void **)&di, sizeof(int), st));
+    PG_TRY(cudaMemcpy2DAsync(dA, (size_t)n * 4, A, (size_t)lda * 4, (size_t)n * 4, n, cudaMemcpyHostToDevice, st));
+    int rc = posit_rpotrf_dev(uplo, n, dA, n, nb, di, st);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(A, (size_t)lda * 4, dA, (size_t)n * 4, (size_t)n * 4, n,
+                                          cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(info, di, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(e);
+    }
+    cudaFreeAsync(dA, st);
+    cudaFreeAsync(di, st);
+    return finish(st, rc);
+}
+
+int posit_rpotrs(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb)
+{
+    bool upper = same(uplo, 'U');
+    if (!upper && !same(uplo, 'L'))
+        return 1;
+    if (n < 0)
+        return 2;
+    if (nrhs < 0)
+        return 3;
+    if (lda < imax(1, n))
+        return 5;
+    if (ldb < imax(1, n))
+        return 7;
+    if (upper)
+        return POSIT_E_UNSUPPORTED;
+    if (n == 0 || nrhs == 0)
+        return 0;
+    int r = ensure_init();
+    if (r)
+        return r;
+    cudaStream_t st = cudaStreamPerThread;
+    uint32_t *dA = nullptr, *dB = nullptr;
+    PG_TRY(cudaMallocAsync((void **)&dA, (size_t)n * n * 4, st));
+    PG_TRY(cudaMallocAsync((void **)&dB, (size_t)n * nrhs * 4, st));
+    PG_TRY(cudaMemcpy2DAsync(dA, (size_t)n * 4, A, (size_t)lda * 4, (size_t)n * 4, n, cudaMemcpyHostToDevice, st));
+    PG_TRY(cudaMemcpy2DAsync(dB, (size_t)n * 4, B, (size_t)ldb * 4, (size_t)n * 4, nrhs, cudaMemcpyHostToDevice, st));
+    int rc = posit_rpotrs_dev(uplo, n, nrhs, dA, n, dB, n, st);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(B, (size_t)ldb * 4, dB, (size_t)n * 4, (size_t)n * 4, nrhs,
+                                          cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(e);
+    }
+    cudaFreeAsync(dA, st);
+    cudaFreeAsync(dB, st);
+    return finish(st, rc);
+}
+
 int posit_from_double_dev(const double *x, uint32_t *out, size_t n, void *stream)
 {
     int r = ensure_init();
@@ -241,6 +509,8 @@ const char *posit_strerror(int code)
         return "kernel error flag raised (bounded wait expired)";
     case POSIT_E_WORKSPACE:
         return "workspace too small or misaligned";
+    case POSIT_E_UNSUPPORTED:
+        return "variant not implemented on the device";
     case POSIT_E_NOALLOC_LIMIT:
         return "shape needs more scratch than the allocation-free entry point's static array";
     default:

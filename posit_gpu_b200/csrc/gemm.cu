@@ -188,13 +188,21 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
 // columns with ty: the 16-byte shared-memory loads of a warp then hit distinct banks.
 __device__ __forceinline__ int own_off(int t, int q) { return (q >> 1) * 32 + 2 * t + (q & 1); }
 
-template <bool DOT>
+// LOWER: only entries with row >= column are written (tiles wholly above the diagonal
+// exit at once) -- the symmetric trailing update of a lower Cholesky factorization.
+// `stop`, if given, is a device flag (a factorization's info) that turns the call into a
+// no-op when it is nonzero.
+template <bool DOT, bool LOWER>
 __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     gemm_main_kernel(int m, int n, int k, int KT, uint32_t alpha, uint32_t beta,
                      const uint2 *__restrict__ Ad, const uint2 *__restrict__ Td, uint32_t *__restrict__ C,
                      size_t ldc, const unsigned char *__restrict__ row_nar,
-                     const unsigned char *__restrict__ col_nar)
+                     const unsigned char *__restrict__ col_nar, const int *__restrict__ stop)
 {
+    if (stop && *stop != 0)
+        return;
+    if (LOWER && (int)(blockIdx.x * BM + BM - 1) < (int)(blockIdx.y * BN))
+        return; // every row of the tile is above its first column
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint2 *As = reinterpret_cast<uint2 *>(smem_raw);
     uint2 *Ts = As + STAGES * BK * BM;
@@ -332,7 +340,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int row = mt * BM + own_off(tx, i), col = nt * BN + own_off(ty, j);
-            if (row < m && col < n) {
+            if (row < m && col < n && (!LOWER || row >= col)) {
                 uint32_t *cp = C + (size_t)row + (size_t)col * ldc;
                 const bool nar = ((nar_bits >> (i * TN + j)) & 1u) || row_nar[row] || col_nar[col];
                 uint32_t v = nar ? P32_NAR : encode(acc[i][j]);
@@ -439,9 +447,10 @@ static int grid_for(size_t total, int threads)
     return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
-cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
-                        int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
-                        void *workspace, cudaStream_t stream)
+template <bool LOWER>
+static cudaError_t gemm_launch_impl(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                                    int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
+                                    void *workspace, cudaStream_t stream, const int *stop)
 {
     GemmPlan p = gemm_plan(m, n, k);
     uint2 *Ad = reinterpret_cast<uint2 *>(workspace);
@@ -458,20 +467,20 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
                                                            Td, col_nar);
     const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2) + (size_t)RT_N * sizeof(RegimeEntry);
     dim3 grid(p.mt, p.nt);
-    e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem)
-                        : cudaFuncSetAttribute(gemm_main_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem);
+    e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem)
+            : cudaFuncSetAttribute(gemm_main_kernel<false, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
     if (e != cudaSuccess)
         return e;
     const bool prof = g_prof_on;
     cudaEvent_t e0 = prof ? prof_mark(stream) : nullptr;
     if (dot)
-        gemm_main_kernel<true><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C, (size_t)ldc,
-                                                                 row_nar, col_nar);
+        gemm_main_kernel<true, LOWER><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
+                                                                        (size_t)ldc, row_nar, col_nar, stop);
     else
-        gemm_main_kernel<false><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
-                                                                  (size_t)ldc, row_nar, col_nar);
+        gemm_main_kernel<false, LOWER><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
+                                                                         (size_t)ldc, row_nar, col_nar, stop);
     if (prof) {
         cudaEvent_t e1 = prof_mark(stream);
         std::lock_guard<std::mutex> lk(g_prof_mu);
@@ -479,6 +488,22 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
     }
     prof_count(3);
     return cudaGetLastError();
+}
+
+cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A, int lda,
+                        const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *workspace,
+                        cudaStream_t stream)
+{
+    return gemm_launch_impl<false>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
+                                   nullptr);
+}
+
+cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A, int lda,
+                              const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *workspace,
+                              cudaStream_t stream, const int *stop)
+{
+    return gemm_launch_impl<true>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
+                                  stop);
 }
 
 cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream)

@@ -36,6 +36,12 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
                         const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
                         uint32_t *C, int ldc, void *workspace, cudaStream_t stream);
 
+// Same, writing only the entries on or below the diagonal of C (row >= column), and
+// doing nothing when *stop != 0 (stop may be null).
+cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_t alpha,
+                              const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
+                              uint32_t *C, int ldc, void *workspace, cudaStream_t stream, const int *stop);
+
 // C <- 0 or beta*C on the m x n submatrix (alpha == 0 or k == 0 with beta != 1).
 cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream);
 

@@ -1,0 +1,470 @@
+// lapack.cu -- device-resident posit32 LU (Rgetrf) and Cholesky (Rpotrf), and their
+// solves (Rgetrs, Rpotrs), bit-exact against the reference's CPU routines.
+//
+// Operation order.  In the reference every entry of L and U receives its updates as
+// a <- a + (-u)*l (Rgemm's c + (alpha*b)*a with alpha = -1, Rgemm.cpp:180-182; Rtrsm's
+// b - b_k*a, Rtrsm.cpp:151, is the same bits because posit multiplication is symmetric in
+// sign) in ascending k, however Rgetrf/Rgetrf2/Rpotrf/Rpotrf2 group the columns into
+// blocks; L entries are then multiplied by the reciprocal of the pivot (Rgetrf2.cpp:121-122,
+// Rscal) or of the Cholesky diagonal (Rtrsm.cpp:265-268), diagonals of a Cholesky factor
+// take a square root (Rpotrf2.cpp:97).  So LU and lower Cholesky are independent of the
+// block size bit for bit (the zero-multiplier skips of Rtrsm/Rsyrk add zero and change
+// nothing unless a NaR is present), and the device code may block the work its own way:
+//
+//   panel (nb columns)   one kernel per column: pivot search + row interchange
+//                        (LU only, one CTA), then scale the column and apply the rank-1
+//                        update to the rest of the panel (all rows in parallel);
+//   U block row          Rtrsm("L","L","N","U") as one CTA per column;
+//   row interchanges     Rlaswp on the columns outside the panel;
+//   trailing update      the posit32 GEMM of gemm.cu (NN for LU; NT restricted to the
+//                        lower triangle for Cholesky).
+// The matrix never leaves the device.  Upper Cholesky (dot-then-combine order, block size
+// dependent) is not implemented on the device.
+#include "gemm.cuh"
+#include "lapack.cuh"
+#include "posit32.cuh"
+
+namespace pg {
+
+// ---------------------------------------------------------------------------
+// LU panel
+// ---------------------------------------------------------------------------
+// Pivot decision of one column, shared by the two kernels of a panel step.
+struct PivotInfo {
+    int row;       // panel-local row of the pivot
+    uint32_t piv;  // pivot value (after the interchange it sits at row k)
+    int mode;      // 0: zero pivot (no scaling), 1: multiply by reciprocal, 2: divide
+    uint32_t recip;
+};
+
+// iRamax (iRamax.cpp:65-71) over panel-local rows [k, M) of column k: the first index of
+// the strict maximum of abs() in posit order (signed integer order of the patterns, NaR
+// lowest), then the interchange of rows k and p over the panel's jb columns
+// (Rgetrf2.cpp:107-117) and the scaling decision (Rgetrf2.cpp:119-131).
+__global__ void lu_pivot_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k, int row0,
+                                int *__restrict__ ipiv, int *__restrict__ info, PivotInfo *__restrict__ pinfo)
+{
+    __shared__ int32_t s_key[1024];
+    __shared__ int s_idx[1024];
+    if (*info < 0)
+        return; // an earlier failure stops the factorization
+    const int tid = threadIdx.x;
+    int32_t best = INT32_MIN;
+    int bidx = -1;
+    const uint32_t *col = P + (size_t)k * lda;
+    for (int i = k + tid; i < M; i += blockDim.x) {
+        int32_t key = (int32_t)pabs(col[i]);
+        if (bidx < 0 || key > best) { // rows visited in increasing order per thread
+            best = key;
+            bidx = i;
+        }
+    }
+    s_key[tid] = best;
+    s_idx[tid] = bidx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (tid < s) {
+            int32_t k2 = s_key[tid + s];
+            int i2 = s_idx[tid + s];
+            bool take = i2 >= 0 && (s_idx[tid] < 0 || k2 > s_key[tid] || (k2 == s_key[tid] && i2 < s_idx[tid]));
+            if (take) {
+                s_key[tid] = k2;
+                s_idx[tid] = i2;
+            }
+        }
+        __syncthreads();
+    }
+    const int p = s_idx[0];
+    const uint32_t piv = col[p];
+    if (tid == 0) {
+        ipiv[row0 + k] = row0 + p + 1; // 1-based, global
+        PivotInfo pi;
+        pi.row = p;
+        pi.piv = piv;
+        if (piv == 0) {
+            pi.mode = 0;
+            pi.recip = 0;
+            if (*info == 0)
+                *info = row0 + k + 1;
+        } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
+            pi.mode = 1;
+            pi.recip = pdiv(P32_ONE, piv);
+        } else {
+            pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
+            pi.recip = 0;
+        }
+        *pinfo = pi;
+    }
+    __syncthreads(); // every thread has read the pivot before the rows move
+    if (piv != 0 && p != k) {
+        for (int c = tid; c < jb; c += blockDim.x) {
+            uint32_t *pc = P + (size_t)c * lda;
+            uint32_t t = pc[k];
+            pc[k] = pc[p];
+            pc[p] = t;
+        }
+    }
+}
+
+// Scale column k below the pivot and apply the rank-1 update to panel columns k+1..jb-1
+// for rows k+1..M-1.  Each thread owns one row; the pivot row (row k, after the
+// interchange) is staged in shared memory.
+__global__ void lu_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
+                                 const int *__restrict__ info, const PivotInfo *__restrict__ pinfo)
+{
+    extern __shared__ uint32_t s_u[]; // -u_kc for c in (k, jb)
+    if (*info < 0)
+        return;
+    const PivotInfo pi = *pinfo;
+    for (int c = k + 1 + threadIdx.x; c < jb; c += blockDim.x)
+        s_u[c - k - 1] = pneg(P[k + (size_t)c * lda]);
+    __syncthreads();
+    const int i = k + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M)
+        return;
+    uint32_t *pk = P + (size_t)k * lda;
+    uint32_t l = pk[i];
+    if (pi.mode == 1)
+        l = pmul(pi.recip, l); // Rscal: da*dx
+    else if (pi.mode == 2)
+        l = pdiv(l, pi.piv);
+    pk[i] = l;
+    for (int c = k + 1; c < jb; ++c) {
+        uint32_t *pc = P + (size_t)c * lda + i;
+        *pc = padd(*pc, pmul(s_u[c - k - 1], l));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rlaswp (Rlaswp.cpp:77-107): interchanges k1..k2 (1-based, global ipiv) applied in order
+// to `ncols` columns starting at A; one thread per column.
+// ---------------------------------------------------------------------------
+__global__ void laswp_kernel(uint32_t *__restrict__ A, size_t lda, int ncols, int k1, int k2,
+                             const int *__restrict__ ipiv, int incx, const int *__restrict__ info)
+{
+    if (info && *info < 0)
+        return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols)
+        return;
+    uint32_t *col = A + (size_t)c * lda;
+    if (incx > 0) {
+        for (int i = k1; i <= k2; ++i) {
+            int ip = ipiv[i - 1];
+            if (ip != i) {
+                uint32_t t = col[i - 1];
+                col[i - 1] = col[ip - 1];
+                col[ip - 1] = t;
+            }
+        }
+    } else {
+        for (int i = k2; i >= k1; --i) {
+            int ip = ipiv[i - 1];
+            if (ip != i) {
+                uint32_t t = col[i - 1];
+                col[i - 1] = col[ip - 1];
+                col[ip - 1] = t;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Triangular solves with many right-hand sides: one CTA per column of B, one thread per
+// row (strided), the column in shared memory.  Loop orders and zero skips as in
+// Rtrsm.cpp:115-156 (side = L, trans = N).
+// ---------------------------------------------------------------------------
+// lower, unit or non-unit diagonal: forward substitution (Rtrsm.cpp:139-154)
+__global__ void trsm_lln_kernel(const uint32_t *__restrict__ L, size_t ldl, uint32_t *__restrict__ B, size_t ldb,
+                                int m, bool unit, const int *__restrict__ info)
+{
+    extern __shared__ uint32_t s_b[];
+    if (info && *info < 0)
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        s_b[i] = bcol[i];
+    __syncthreads();
+    for (int k = 0; k < m; ++k) {
+        uint32_t bk = s_b[k];
+        if (bk != 0) {
+            if (!unit) {
+                bk = pdiv(bk, L[k + (size_t)k * ldl]);
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    s_b[k] = bk;
+            }
+            const uint32_t nb = pneg(bk);
+            for (int i = k + 1 + threadIdx.x; i < m; i += blockDim.x)
+                s_b[i] = padd(s_b[i], pmul(nb, L[i + (size_t)k * ldl]));
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        bcol[i] = s_b[i];
+}
+
+// upper, non-unit diagonal: backward substitution (Rtrsm.cpp:121-136)
+__global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint32_t *__restrict__ B, size_t ldb,
+                                int m, bool unit, const int *__restrict__ info)
+{
+    extern __shared__ uint32_t s_b[];
+    if (info && *info < 0)
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        s_b[i] = bcol[i];
+    __syncthreads();
+    for (int k = m - 1; k >= 0; --k) {
+        uint32_t bk = s_b[k];
+        if (bk != 0) {
+            if (!unit) {
+                bk = pdiv(bk, U[k + (size_t)k * ldu]);
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    s_b[k] = bk;
+            }
+            const uint32_t nb = pneg(bk);
+            for (int i = threadIdx.x; i < k; i += blockDim.x)
+                s_b[i] = padd(s_b[i], pmul(nb, U[i + (size_t)k * ldu]));
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        bcol[i] = s_b[i];
+}
+
+// Lower, transposed, non-unit (Rtrsm.cpp:175-186): for i = m-1..0,
+// t = b_i - sum_{k>i} a_ki*b_k (k ascending), b_i = t / a_ii.  Each b_i's sum starts with
+// the b_{i+1} just computed, so the whole solve is one dependent chain; the products
+// are computed by the CTA ahead of the chain and one thread runs the chain of additions.
+__global__ void trsm_llt_kernel(const uint32_t *__restrict__ L, size_t ldl, uint32_t *__restrict__ B, size_t ldb,
+                                int m, bool unit, const int *__restrict__ info)
+{
+    extern __shared__ uint32_t s_b[]; // [0, m): b; [m, 2m): products of the current row
+    if (info && *info < 0)
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    uint32_t *s_p = s_b + m;
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        s_b[i] = bcol[i];
+    __syncthreads();
+    for (int i = m - 1; i >= 0; --i) {
+        const uint32_t *li = L + (size_t)i * ldl; // column i of L: a_ki for k > i
+        for (int k = i + 1 + threadIdx.x; k < m; k += blockDim.x)
+            s_p[k] = pmul(li[k], s_b[k]);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = s_b[i]; // alpha*b with alpha == 1
+            for (int k = i + 1; k < m; ++k)
+                t = psub(t, s_p[k]);
+            if (!unit)
+                t = pdiv(t, li[i]);
+            s_b[i] = t;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        bcol[i] = s_b[i];
+}
+
+// ---------------------------------------------------------------------------
+// Cholesky panel (lower)
+// ---------------------------------------------------------------------------
+// Step k of the panel whose top-left corner is the diagonal entry (row0, row0), in two
+// kernels.  chol_diag_kernel (one CTA): l_kk = sqrt(a_kk) -- a_kk <= 0 in posit order, NaR
+// included, stops with info (Rpotrf2.cpp:90-93) -- and l_ck = (1/l_kk)*a_ck for the rows
+// c in (k, jb) of the panel's diagonal block (Rtrsm.cpp:265-268).  chol_update_kernel:
+// l_ik = (1/l_kk)*a_ik for the rows below the diagonal block, then the rank-1 update of
+// the panel's lower part, a_ic += (-l_ck)*l_ik for k < c <= i, rows in parallel.
+__global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int jb, int k, int row0,
+                                 int *__restrict__ info, uint32_t *__restrict__ recip_out)
+{
+    __shared__ uint32_t s_recip;
+    __shared__ int s_stop;
+    if (*info != 0)
+        return;
+    uint32_t *pk = P + (size_t)k * lda;
+    if (threadIdx.x == 0) {
+        uint32_t akk = pk[k];
+        s_stop = (int32_t)akk <= 0;
+        if (s_stop) {
+            *info = row0 + k + 1;
+        } else {
+            uint32_t lkk = psqrt(akk);
+            s_recip = pdiv(P32_ONE, lkk);
+            pk[k] = lkk;
+            *recip_out = s_recip;
+        }
+    }
+    __syncthreads();
+    if (s_stop)
+        return;
+    for (int c = k + 1 + threadIdx.x; c < jb; c += blockDim.x)
+        pk[c] = pmul(s_recip, pk[c]);
+}
+
+__global__ void chol_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
+                                   const int *__restrict__ info, const uint32_t *__restrict__ recip_in)
+{
+    extern __shared__ uint32_t s_l[]; // -l_ck for c in (k, jb)
+    if (*info != 0)
+        return;
+    const uint32_t *pk = P + (size_t)k * lda;
+    for (int c = k + 1 + threadIdx.x; c < jb; c += blockDim.x)
+        s_l[c - k - 1] = pneg(pk[c]);
+    __syncthreads();
+    const int i = k + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M)
+        return;
+    uint32_t l = pk[i];
+    if (i >= jb) { // rows of the diagonal block were scaled by chol_diag_kernel
+        l = pmul(*recip_in, l);
+        P[(size_t)k * lda + i] = l;
+    }
+    const int cmax = min(jb - 1, i);
+    for (int c = k + 1; c <= cmax; ++c) {
+        uint32_t *pc = P + (size_t)c * lda + i;
+        *pc = padd(*pc, pmul(s_l[c - k - 1], l));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------
+static int imin(int a, int b) { return a < b ? a : b; }
+
+size_t rgetrf_workspace_bytes(int m, int n, int nb)
+{
+    int mn = imin(m, n);
+    if (nb < 1)
+        nb = 1;
+    int jb = imin(nb, mn);
+    size_t g = mn > jb ? gemm_workspace_bytes(m - jb > 0 ? m - jb : 1, n - jb > 0 ? n - jb : 1, jb) : 0;
+    return 256 + g;
+}
+
+// Rgetrf.cpp:95-132 with the device kernels above.  `ws` holds a PivotInfo and the
+// trailing GEMM's workspace.
+cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *ws,
+                          cudaStream_t st)
+{
+    const int mn = imin(m, n);
+    if (nb < 1)
+        nb = 1;
+    PivotInfo *pinfo = reinterpret_cast<PivotInfo *>(ws);
+    void *gws = reinterpret_cast<unsigned char *>(ws) + 256;
+    const size_t L = (size_t)lda;
+    for (int j = 0; j < mn; j += nb) {
+        const int jb = imin(mn - j, nb);
+        const int M = m - j;
+        uint32_t *P = A + j + (size_t)j * L;
+        for (int k = 0; k < jb; ++k) {
+            lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k, j, ipiv, info, pinfo);
+            const int rows = M - k - 1;
+            if (rows > 0 || k + 1 < jb) {
+                const int blocks = rows > 0 ? (rows + 255) / 256 : 1;
+                lu_update_kernel<<<blocks, 256, (size_t)jb * 4, st>>>(P, L, M, jb, k, info, pinfo);
+            }
+        }
+        if (j > 0)
+            laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
+        if (j + jb < n) {
+            const int nr = n - j - jb;
+            uint32_t *A12 = A + j + (size_t)(j + jb) * L;
+            laswp_kernel<<<(nr + 127) / 128, 128, 0, st>>>(A + (size_t)(j + jb) * L, L, nr, j + 1, j + jb, ipiv, 1,
+                                                          info);
+            trsm_lln_kernel<<<nr, 256, (size_t)jb * 4, st>>>(P, L, A12, L, jb, true, info);
+            if (j + jb < m) {
+                cudaError_t e = gemm_launch(true, true, m - j - jb, nr, jb, 0xC0000000u /* -1 */,
+                                            A + (j + jb) + (size_t)j * L, lda, A12, lda, P32_ONE,
+                                            A + (j + jb) + (size_t)(j + jb) * L, lda, gws, st);
+                if (e != cudaSuccess)
+                    return e;
+            }
+        }
+    }
+    return cudaGetLastError();
+}
+
+size_t rpotrf_workspace_bytes(int n, int nb)
+{
+    if (nb < 1)
+        nb = 1;
+    int jb = imin(nb, n);
+    return 256 + (n > jb ? gemm_workspace_bytes(n - jb, n - jb, jb) : 0);
+}
+
+// Lower Cholesky (Rpotrf.cpp:124-142 / Rpotrf2.cpp:132-146 order, blocked right-looking).
+cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st)
+{
+    if (nb < 1)
+        nb = 1;
+    void *gws = reinterpret_cast<unsigned char *>(ws) + 256;
+    const size_t L = (size_t)lda;
+    for (int j = 0; j < n; j += nb) {
+        const int jb = imin(n - j, nb);
+        const int M = n - j;
+        uint32_t *P = A + j + (size_t)j * L;
+        uint32_t *recip = reinterpret_cast<uint32_t *>(ws);
+        for (int k = 0; k < jb; ++k) {
+            chol_diag_kernel<<<1, 256, 0, st>>>(P, L, jb, k, j, info, recip);
+            const int rows = M - k - 1;
+            if (rows > 0) {
+                const int blocks = (rows + 255) / 256;
+                chol_update_kernel<<<blocks, 256, (size_t)jb * 4, st>>>(P, L, M, jb, k, info, recip);
+            }
+        }
+        if (j + jb < n) {
+            const int nr = n - j - jb;
+            const uint32_t *L21 = A + (j + jb) + (size_t)j * L;
+            cudaError_t e = gemm_launch_lower(false, false, nr, nr, jb, 0xC0000000u /* -1 */, L21, lda, L21,
+                                              lda, P32_ONE, A + (j + jb) + (size_t)(j + jb) * L, lda, gws, st, info);
+            if (e != cudaSuccess)
+                return e;
+        }
+    }
+    return cudaGetLastError();
+}
+
+// Rgetrs.cpp:84-114 (trans = 'N'): interchanges, L (unit) forward, U backward.
+static cudaError_t solve_smem(size_t bytes)
+{
+    if (bytes <= 48 * 1024)
+        return cudaSuccess;
+    if (bytes > 227 * 1024)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(trsm_lln_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(trsm_lun_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(trsm_llt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return e;
+}
+
+cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb,
+                          cudaStream_t st)
+{
+    const int threads = 1024;
+    cudaError_t e = solve_smem((size_t)n * 4);
+    if (e != cudaSuccess)
+        return e;
+    laswp_kernel<<<(nrhs + 127) / 128, 128, 0, st>>>(B, ldb, nrhs, 1, n, ipiv, 1, nullptr);
+    trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, true, nullptr);
+    trsm_lun_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
+    return cudaGetLastError();
+}
+
+// Rpotrs.cpp:95-106 (uplo = 'L'): L forward, L^T backward.
+cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
+{
+    const int threads = 1024;
+    cudaError_t e = solve_smem((size_t)n * 8);
+    if (e != cudaSuccess)
+        return e;
+    trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
+    trsm_llt_kernel<<<nrhs, threads, (size_t)n * 8, st>>>(A, lda, B, ldb, n, false, nullptr);
+    return cudaGetLastError();
+}
+
+} // namespace pg

@@ -1,0 +1,22 @@
+// lapack.cuh -- device-resident posit32 factorizations and solves (lapack.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pg {
+
+size_t rgetrf_workspace_bytes(int m, int n, int nb);
+size_t rpotrf_workspace_bytes(int n, int nb);
+
+// All pointers are device pointers; ipiv is 1-based as in the reference; *info must be
+// zero on entry (it receives the first zero pivot / the first non-positive diagonal).
+cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *ws,
+                          cudaStream_t st);
+cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st);
+cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb,
+                          cudaStream_t st);
+cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb,
+                                cudaStream_t st);
+
+} // namespace pg
