@@ -8,7 +8,7 @@
 #include <mpblas.h>
 #include <mplapack.h>
 
-void ref_set_nb(int nb);
+extern "C" void ref_set_nb(int nb);
 
 static inline posit32 *PP(uint32_t *u) { return reinterpret_cast<posit32 *>(u); }
 

@@ -418,7 +418,7 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         if (j + jb < n) {
             const int nr = n - j - jb;
             const uint32_t *L21 = A + (j + jb) + (size_t)j * L;
-            cudaError_t e = gemm_launch_lower(false, false, nr, nr, jb, 0xC0000000u /* -1 */, L21, lda, L21,
+            cudaError_t e = gemm_launch_lower(true, false, nr, nr, jb, 0xC0000000u /* -1 */, L21, lda, L21,
                                               lda, P32_ONE, A + (j + jb) + (size_t)(j + jb) * L, lda, gws, st, info);
             if (e != cudaSuccess)
                 return e;
