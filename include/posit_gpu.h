@@ -80,7 +80,11 @@ size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
  * for inputs without NaR).  Return value: 0, the number of an illegal argument (as the
  * reference passes to Mxerbla: 1, 2, 4, ... ), or a negative POSIT_E_* code.  The
  * numerical result goes to *info exactly as in the reference (first zero pivot / first
- * non-positive leading minor, 1-based; 0 on success).  nb <= 0 selects 256.
+ * non-positive leading minor, 1-based; 0 on success).  LU continues past a zero pivot as
+ * the reference does, and its factors stay bit-identical; a Cholesky factorization that
+ * stops (info > 0) leaves the not-yet-factored part of A in an unspecified state (the
+ * reference's left-looking blocking and this right-looking one differ there).
+ * nb <= 0 selects 256.
  *
  * _dev forms: device pointers (ipiv and info included: *info is written on the device,
  * asynchronously on `stream`); workspace is stream-ordered.  Host forms: host pointers,
@@ -100,6 +104,32 @@ int posit_rpotrf(char uplo, int n, uint32_t *A, int lda, int nb, int *info);
 /* Rpotrs (libRpack/Rpotrs.cpp:32-110; mplapack_posit.h:97) */
 int posit_rpotrs_dev(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, void *stream);
 int posit_rpotrs(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb);
+
+/* ---- Batched factor-and-solve (no reference counterpart) ---------------------------
+ * Many independent LU or Cholesky problems, each factored in place and solved for its
+ * right-hand sides, in ONE persistent kernel fed by a device work queue (largest
+ * problems first), captured once in a CUDA graph.  Results are bit-identical to the
+ * per-call path (posit_rgetrf_dev + posit_rgetrs_dev, posit_rpotrf_dev('L') +
+ * posit_rpotrs_dev('L')) and hence to the CPU routines.  Each problem runs on one thread
+ * block, so this is for many small-to-medium problems (n <= POSIT_BATCH_MAX_N). */
+#define POSIT_BATCH_LU 0
+#define POSIT_BATCH_CHOLESKY 1
+#define POSIT_BATCH_MAX_N 4096
+typedef struct {
+    int kind;           /* POSIT_BATCH_LU or POSIT_BATCH_CHOLESKY (lower) */
+    int n, lda, nrhs, ldb;
+    uint32_t *A;        /* device, n x n, factored in place */
+    uint32_t *B;        /* device, n x nrhs, overwritten by the solution */
+    int *ipiv;          /* device, n 1-based pivots (LU only) */
+    int *info;          /* device, the reference's info */
+} posit_batch_problem;
+typedef struct posit_batch_plan posit_batch_plan;
+/* Uploads the descriptors (host array) and captures the launch; returns 0, 1/2 for bad
+ * arguments / a bad descriptor, or POSIT_E_*. */
+int posit_batch_plan_create(const posit_batch_problem *probs, int nprob, posit_batch_plan **plan);
+/* Replays the captured launch on `stream` (asynchronous). */
+int posit_batch_plan_launch(posit_batch_plan *plan, void *stream);
+void posit_batch_plan_destroy(posit_batch_plan *plan);
 
 /* Element-wise conversions on device buffers, asynchronous on `stream`.
  * Replace the SoftPosit class conversions the reference drivers use to build their

@@ -235,6 +235,63 @@ def Rpotrs_dev(uplo, n, nrhs, A, lda, B, ldb, stream=None):
                                  _stream_of(A, stream)), "Rpotrs")
 
 
+# ---------------------------------------------------------------------------
+# Batched factor-and-solve: one persistent launch, captured in a CUDA graph
+# ---------------------------------------------------------------------------
+BATCH_LU = 0
+BATCH_CHOLESKY = 1
+BATCH_MAX_N = 4096
+
+
+class _BatchProblem(_c.Structure):
+    _fields_ = [("kind", _c.c_int), ("n", _c.c_int), ("lda", _c.c_int), ("nrhs", _c.c_int), ("ldb", _c.c_int),
+                ("A", _VP), ("B", _VP), ("ipiv", _VP), ("info", _VP)]
+
+
+_lib.posit_batch_plan_create.argtypes = [_c.POINTER(_BatchProblem), _c.c_int, _c.POINTER(_VP)]
+_lib.posit_batch_plan_create.restype = _c.c_int
+_lib.posit_batch_plan_launch.argtypes = [_VP, _VP]
+_lib.posit_batch_plan_launch.restype = _c.c_int
+_lib.posit_batch_plan_destroy.argtypes = [_VP]
+
+
+class BatchPlan:
+    """Factor-and-solve many problems in one graph-captured persistent launch.
+
+    problems: iterable of (kind, A, B, ipiv, info) with kind BATCH_LU / BATCH_CHOLESKY,
+    A an n x n column-major CUDA tensor of 4-byte posit patterns (flat or 2-D), B its
+    n x nrhs right-hand sides (flat, column-major), ipiv an int32 CUDA tensor of n
+    entries (LU; may be None for Cholesky), info an int32 CUDA tensor of one entry.
+    The tensors must stay alive while the plan is used."""
+
+    def __init__(self, problems):
+        probs = list(problems)
+        arr = (_BatchProblem * max(1, len(probs)))()
+        self._keep = []
+        for i, (kind, A, B, ipiv, info) in enumerate(probs):
+            n = int(round(A.numel() ** 0.5))
+            if n * n != A.numel():
+                raise ValueError("A must be square")
+            nrhs = B.numel() // n if n else 0
+            arr[i] = _BatchProblem(kind, n, max(1, n), nrhs, max(1, n), A.data_ptr(), B.data_ptr(),
+                                   ipiv.data_ptr() if ipiv is not None else None, info.data_ptr())
+            self._keep.append((A, B, ipiv, info))
+        h = _VP()
+        _check(_lib.posit_batch_plan_create(arr, len(probs), _c.byref(h)), "batch plan")
+        self._h = h
+
+    def launch(self, stream=None):
+        import torch
+        st = stream or torch.cuda.current_stream()
+        _check(_lib.posit_batch_plan_launch(self._h, st.cuda_stream), "batch launch")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.posit_batch_plan_destroy(h)
+            self._h = None
+
+
 NOALLOC_SCRATCH_BYTES = 64 << 20
 POSIT_E_NOALLOC_LIMIT = -6
 

@@ -1,0 +1,268 @@
+// batch.cu -- many independent posit32 LU / Cholesky factor-and-solve problems in one
+// persistent launch fed by a device work queue.
+//
+// Each CTA takes the next problem from the queue (an atomic counter over a list sorted by
+// decreasing size, so the largest problems start first) and factors and solves it alone:
+// right-looking, one column per step, the matrix and right-hand sides in global memory
+// (L2-resident for the sizes batched here).  Per-element operation order is the
+// reference's (see lapack.cu), so every factor, pivot and solution is bit-identical to
+// the per-call path (posit_rgetrf_dev + posit_rgetrs_dev, posit_rpotrf_dev +
+// posit_rpotrs_dev) and to the CPU routines.
+#include "batch.cuh"
+#include "posit32.cuh"
+
+namespace pg {
+
+namespace {
+
+constexpr int BT = 256; // threads per problem
+
+__device__ int iramax_block(const uint32_t *col, int k, int n, int32_t *s_key, int *s_idx)
+{
+    const int tid = threadIdx.x;
+    int32_t best = INT32_MIN;
+    int bidx = -1;
+    for (int i = k + tid; i < n; i += blockDim.x) {
+        int32_t key = (int32_t)pabs(col[i]);
+        if (bidx < 0 || key > best) {
+            best = key;
+            bidx = i;
+        }
+    }
+    s_key[tid] = best;
+    s_idx[tid] = bidx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (tid < s) {
+            int32_t k2 = s_key[tid + s];
+            int i2 = s_idx[tid + s];
+            if (i2 >= 0 && (s_idx[tid] < 0 || k2 > s_key[tid] || (k2 == s_key[tid] && i2 < s_idx[tid]))) {
+                s_key[tid] = k2;
+                s_idx[tid] = i2;
+            }
+        }
+        __syncthreads();
+    }
+    int p = s_idx[0];
+    __syncthreads();
+    return p;
+}
+
+// Rgetrf (as unblocked right-looking LU) + Rgetrs('N') for one problem.
+__device__ void lu_solve_one(const BatchProblem &pr, int32_t *s_key, int *s_idx, uint32_t *s_row)
+{
+    const int n = pr.n, tid = threadIdx.x;
+    uint32_t *A = pr.A;
+    const size_t lda = (size_t)pr.lda;
+    int info = 0;
+    __shared__ uint32_t s_piv, s_recip;
+    __shared__ int s_mode;
+    for (int k = 0; k < n; ++k) {
+        uint32_t *ck = A + (size_t)k * lda;
+        const int p = iramax_block(ck, k, n, s_key, s_idx);
+        const uint32_t piv = ck[p];
+        if (tid == 0) {
+            pr.ipiv[k] = p + 1;
+            if (piv == 0) {
+                s_mode = 0;
+            } else if ((int32_t)pabs(piv) >= 1) {
+                s_mode = 1;
+                s_recip = pdiv(P32_ONE, piv);
+            } else {
+                s_mode = 2;
+            }
+            s_piv = piv;
+        }
+        if (piv == 0 && info == 0)
+            info = k + 1;
+        __syncthreads();
+        if (piv != 0 && p != k) { // interchange whole rows (Rlaswp on both sides)
+            for (int c = tid; c < n; c += blockDim.x) {
+                uint32_t *pc = A + (size_t)c * lda;
+                uint32_t t = pc[k];
+                pc[k] = pc[p];
+                pc[p] = t;
+            }
+        }
+        __syncthreads();
+        const int mode = s_mode;
+        for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+            uint32_t l = ck[i];
+            if (mode == 1)
+                l = pmul(s_recip, l);
+            else if (mode == 2)
+                l = pdiv(l, s_piv);
+            ck[i] = l;
+        }
+        for (int c = k + 1 + tid; c < n; c += blockDim.x)
+            s_row[c] = pneg(A[k + (size_t)c * lda]);
+        __syncthreads();
+        const int rows = n - k - 1;
+        const int cnt = rows * rows;
+        for (int e = tid; e < cnt; e += blockDim.x) {
+            const int i = k + 1 + e % rows, c = k + 1 + e / rows;
+            uint32_t *pc = A + i + (size_t)c * lda;
+            *pc = padd(*pc, pmul(s_row[c], ck[i]));
+        }
+        __syncthreads();
+    }
+    if (tid == 0)
+        *pr.info = info;
+    // Rgetrs 'N': interchanges, L (unit) forward, U backward -- per right-hand side
+    for (int r = 0; r < pr.nrhs; ++r) {
+        uint32_t *b = pr.B + (size_t)r * pr.ldb;
+        if (tid == 0)
+            for (int i = 0; i < n; ++i) {
+                int ip = pr.ipiv[i] - 1;
+                if (ip != i) {
+                    uint32_t t = b[i];
+                    b[i] = b[ip];
+                    b[ip] = t;
+                }
+            }
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            const uint32_t bk = b[k];
+            if (bk != 0) {
+                const uint32_t nb = pneg(bk);
+                const uint32_t *lk = A + (size_t)k * lda;
+                for (int i = k + 1 + tid; i < n; i += blockDim.x)
+                    b[i] = padd(b[i], pmul(nb, lk[i]));
+            }
+            __syncthreads();
+        }
+        for (int k = n - 1; k >= 0; --k) {
+            uint32_t bk = b[k];
+            __syncthreads();
+            if (bk != 0) {
+                const uint32_t *uk = A + (size_t)k * lda;
+                bk = pdiv(bk, uk[k]);
+                if (tid == 0)
+                    b[k] = bk;
+                const uint32_t nb = pneg(bk);
+                for (int i = tid; i < k; i += blockDim.x)
+                    b[i] = padd(b[i], pmul(nb, uk[i]));
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Rpotrf('L') (as unblocked right-looking Cholesky) + Rpotrs('L') for one problem.
+__device__ void chol_solve_one(const BatchProblem &pr, uint32_t *s_row)
+{
+    const int n = pr.n, tid = threadIdx.x;
+    uint32_t *A = pr.A;
+    const size_t lda = (size_t)pr.lda;
+    __shared__ uint32_t s_recip;
+    __shared__ int s_fail;
+    int info = 0;
+    for (int k = 0; k < n; ++k) {
+        uint32_t *ck = A + (size_t)k * lda;
+        if (tid == 0) {
+            uint32_t akk = ck[k];
+            s_fail = (int32_t)akk <= 0;
+            if (!s_fail) {
+                uint32_t lkk = psqrt(akk);
+                ck[k] = lkk;
+                s_recip = pdiv(P32_ONE, lkk);
+            }
+        }
+        __syncthreads();
+        if (s_fail) {
+            info = k + 1;
+            break;
+        }
+        for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+            const uint32_t l = pmul(s_recip, ck[i]);
+            ck[i] = l;
+            s_row[i] = pneg(l);
+        }
+        __syncthreads();
+        // lower part of the trailing matrix: a_ic += (-l_ck)*l_ik, k < c <= i
+        const int rows = n - k - 1;
+        const int cnt = rows * rows;
+        for (int e = tid; e < cnt; e += blockDim.x) {
+            const int i = k + 1 + e % rows, c = k + 1 + e / rows;
+            if (i >= c) {
+                uint32_t *pc = A + i + (size_t)c * lda;
+                *pc = padd(*pc, pmul(s_row[c], ck[i]));
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0)
+        *pr.info = info;
+    if (info != 0)
+        return;
+    for (int r = 0; r < pr.nrhs; ++r) {
+        uint32_t *b = pr.B + (size_t)r * pr.ldb;
+        // L forward, non-unit: b_k /= l_kk, then b_i -= b_k*l_ik
+        for (int k = 0; k < n; ++k) {
+            uint32_t bk = b[k];
+            __syncthreads();
+            if (bk != 0) {
+                const uint32_t *lk = A + (size_t)k * lda;
+                bk = pdiv(bk, lk[k]);
+                if (tid == 0)
+                    b[k] = bk;
+                const uint32_t nb = pneg(bk);
+                for (int i = k + 1 + tid; i < n; i += blockDim.x)
+                    b[i] = padd(b[i], pmul(nb, lk[i]));
+            }
+            __syncthreads();
+        }
+        // L^T backward: t = b_i - sum_{k>i} l_ki*b_k (k ascending), b_i = t / l_ii
+        for (int i = n - 1; i >= 0; --i) {
+            const uint32_t *li = A + (size_t)i * lda;
+            for (int k = i + 1 + tid; k < n; k += blockDim.x)
+                s_row[k] = pmul(li[k], b[k]);
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t t = b[i];
+                for (int k = i + 1; k < n; ++k)
+                    t = psub(t, s_row[k]);
+                b[i] = pdiv(t, li[i]);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+} // namespace
+
+__global__ void __launch_bounds__(BT) batch_factor_kernel(const BatchProblem *__restrict__ probs, int nprob,
+                                                          const int *__restrict__ order, int *__restrict__ next)
+{
+    __shared__ int32_t s_key[BT];
+    __shared__ int s_idx[BT];
+    __shared__ int s_item;
+    __shared__ uint32_t s_row[BATCH_MAX_N];
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_item = atomicAdd(next, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= nprob)
+            return;
+        const BatchProblem pr = probs[order ? order[item] : item];
+        if (pr.kind == BATCH_LU)
+            lu_solve_one(pr, s_key, s_idx, s_row);
+        else
+            chol_solve_one(pr, s_row);
+        __syncthreads();
+    }
+}
+
+cudaError_t batch_factor_launch(const BatchProblem *probs, int nprob, const int *order, int *next, int ctas,
+                                cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(int), st);
+    if (e != cudaSuccess)
+        return e;
+    batch_factor_kernel<<<ctas, BT, 0, st>>>(probs, nprob, order, next);
+    return cudaGetLastError();
+}
+
+} // namespace pg

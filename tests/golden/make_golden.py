@@ -15,6 +15,9 @@ Outputs:
   lapack.npz  Rgetrf / Rgetrs / Rpotrf / Rpotrs (nb override) on small systems
   hashes.json SHA-256 of Rgemm outputs on larger seeded problems (config-1 512^3 NN and
               a 256^3 case per transpose), with the recipe that regenerates the inputs
+  factor_hashes.json
+              SHA-256 of the reference's Rgetrf/Rgetrs and Rpotrf/Rpotrs results on the
+              seeded n = 1024 and 4096 systems (nb = 256); `... make_golden.py factors`
 """
 import hashlib
 import json
@@ -182,8 +185,65 @@ def make_hashes(ref):
     return len(res)
 
 
+def factor_cases():
+    """Config-3 factorizations: GE U[-1,1] for LU, SPD M*M^T/n + I for Cholesky, nb = 256,
+    b = A*x_true with x_true U[-1,1]."""
+    return [dict(name=f"lu_{n}", kind="lu", n=n, nb=256, seed=3000 + n) for n in (1024, 4096)] + \
+           [dict(name=f"chol_{n}", kind="chol", n=n, nb=256, seed=5000 + n) for n in (1024, 4096)]
+
+
+def regen_factor_inputs(case):
+    """A (column-major n x n) and x_true, from default_rng(seed): for LU A ~ U[-1,1]; for
+    Cholesky M ~ U[-1,1] then A = M*M^T/n + I formed in FP64; then x_true ~ U[-1,1]."""
+    rng = np.random.default_rng(case["seed"])
+    n = case["n"]
+    if case["kind"] == "lu":
+        A = oracle.from_double(rng.uniform(-1.0, 1.0, n * n))
+    else:
+        M = rng.uniform(-1.0, 1.0, (n, n))
+        A = oracle.from_double((M @ M.T / n + np.eye(n)).reshape(-1, order="F"))
+    x = oracle.from_double(rng.uniform(-1.0, 1.0, n))
+    return A, x
+
+
+def make_factor_hashes(ref, names=None):
+    """SHA-256 of the reference's CPU factors, pivots and solutions (can take minutes)."""
+    out_path = os.path.join(OUT, "factor_hashes.json")
+    res = json.load(open(out_path)) if os.path.exists(out_path) else {}
+    for c in factor_cases():
+        if names and c["name"] not in names:
+            continue
+        A, x = regen_factor_inputs(c)
+        n = c["n"]
+        b = np.zeros(n, np.uint32)
+        ref.ref_rgemv(b"N", n, n, oracle.P32_ONE, A, n, x, 1, 0, b, 1)  # b = A*x (Rgemv.cpp:152-162)
+        F = A.copy()
+        rhs = b.copy()
+        if c["kind"] == "lu":
+            ipiv = np.zeros(n, np.int32)
+            info = ref.ref_rgetrf(n, n, F, n, ipiv, c["nb"])
+            ref.ref_rgetrs(b"N", n, 1, F, n, ipiv, rhs, n)
+            extra = {"ipiv_sha256": hashlib.sha256(ipiv.tobytes()).hexdigest()}
+        else:
+            info = ref.ref_rpotrf(b"L", n, F, n, c["nb"])
+            ref.ref_rpotrs(b"L", n, 1, F, n, rhs, n)
+            extra = {}
+        res[c["name"]] = dict(c, info=int(info), A_sha256=hashlib.sha256(A.tobytes()).hexdigest(),
+                              b_sha256=hashlib.sha256(b.tobytes()).hexdigest(),
+                              factor_sha256=hashlib.sha256(F.tobytes()).hexdigest(),
+                              x_sha256=hashlib.sha256(rhs.tobytes()).hexdigest(), **extra)
+        with open(out_path, "w") as f:
+            json.dump(res, f, indent=1)
+        print("factor hash", c["name"], flush=True)
+    return len(res)
+
+
 def main():
+    import sys
     ref = ref_lib()
+    if len(sys.argv) > 1 and sys.argv[1] == "factors":
+        print("factors", make_factor_hashes(ref, sys.argv[2:] or None))
+        return
     print("ops", make_ops(ref))
     print("rgemm", make_rgemm(ref))
     print("lapack", make_lapack(ref))
