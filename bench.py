@@ -52,6 +52,12 @@ def parse():
     ap.add_argument("--trans", default="NN")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="gemm", choices=["gemm", "lu", "cholesky", "batch"],
+                    help="gemm (default, the headline), lu / cholesky (device-resident "
+                         "factorization + solve, FP64 errors), batch (batched vs per-call)")
+    ap.add_argument("--nb", type=int, default=0, help="panel width for lu/cholesky (0: tuned)")
+    ap.add_argument("--problems", type=int, default=20000, help="batch: factor-and-solve problems")
+    ap.add_argument("--gemms", type=int, default=50000, help="batch: GEMM problems")
     return ap.parse_args()
 
 
@@ -334,10 +340,232 @@ def ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# device-resident factorization (configuration 3) and batching (configuration 4)
+# ---------------------------------------------------------------------------
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def factor_arm(args):
+    """LU or Cholesky of one n x n system, nb from the tuner: posit Gop/s with the
+    reference's work formulas ((2/3)n^3 LU, (1/3)n^3 Cholesky; main_lu_bench.cpp:102,
+    main_cholesky_bench.cpp:113), the solve, and the FP64 error report."""
+    import torch
+
+    import posit_gpu_b200 as pg
+    from posit_gpu_b200 import accuracy, autotune
+    n = args.n
+    lu = args.workload == "lu"
+    nb = args.nb or autotune.panel_width(n, "lu" if lu else "chol")
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(4242)
+    if lu:
+        A0 = pg.from_double_dev(torch.rand(n * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    else:
+        M = torch.rand(n, n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        S = M @ M.t() / n + torch.eye(n, dtype=torch.float64, device=dev)
+        A0 = pg.from_double_dev(S.t().contiguous().reshape(-1))
+        del M, S
+    x = pg.from_double_dev(torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    b = torch.zeros(n, dtype=torch.int32, device=dev)
+    pg.Rgemm_dev("N", "N", n, 1, n, pg.P32_ONE, A0, n, x, n, 0, b, n)
+    A = A0.clone()
+    ipiv = torch.zeros(n, dtype=torch.int32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def factor():
+        if lu:
+            pg.Rgetrf_dev(n, n, A, n, ipiv, info, nb=nb)
+        else:
+            pg.Rpotrf_dev("L", n, A, n, info, nb=nb)
+
+    times = []
+    for i in range(args.warmup + args.steps):
+        A.copy_(A0)
+        e0, e1 = _events()
+        e0.record()
+        factor()
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    ms = sum(times) / len(times)
+    rhs = b.clone()
+    e0, e1 = _events()
+    e0.record()
+    if lu:
+        pg.Rgetrs_dev("N", n, 1, A, n, ipiv, rhs, n)
+    else:
+        pg.Rpotrs_dev("L", n, 1, A, n, rhs, n)
+    e1.record()
+    torch.cuda.synchronize()
+    solve_ms = e0.elapsed_time(e1)
+    work = (2.0 if lu else 1.0) / 3.0 * n ** 3
+    rep = accuracy.solve_report(A0, b, rhs, x_true=x, n=n, spd=not lu)
+    line = {"metric": f"posit32 {'Rgetrf' if lu else 'Rpotrf(L)'} Gop/s ({'2/3' if lu else '1/3'} n^3 / t), "
+                      f"device-resident, bit-exact vs CPU", "value": round(work / (ms / 1e3) / 1e9, 3),
+            "unit": "Gop/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "posit32",
+            "data": "synthetic", "config": {"workload": f"{args.workload} n={n} nb={nb}, "
+                                                        f"{'U[-1,1]' if lu else 'M*M^T/n + I, M ~ U[-1,1]'}, "
+                                                        "one right-hand side b = A*x_true"},
+            "info": int(info.item()), "solve_ms": round(solve_ms, 3), "fp64_report": rep}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _logu(rng, lo, hi, size):
+    import numpy as np
+    return np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size))).astype(int)
+
+
+def batch_arm(args):
+    """Configuration 4: 20,000 LU/Cholesky factor-and-solve problems (n log-uniform 8..512)
+    and 50,000 GEMMs (m, n, k log-uniform 4..512, random transposes), batched (one
+    persistent graph-captured launch each) against the plain per-call path on a sample."""
+    import numpy as np
+    import torch
+
+    import posit_gpu_b200 as pg
+    from posit_gpu_b200 import autotune
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(20260101)
+    g = torch.Generator(device=dev)
+    g.manual_seed(99)
+    P = args.problems
+    ns = _logu(rng, 8, 512, P)
+    kinds = np.where(rng.random(P) < 0.5, pg.BATCH_LU, pg.BATCH_CHOLESKY)
+    # one arena per kind of buffer
+    offA = np.concatenate([[0], np.cumsum(ns * ns)])
+    offB = np.concatenate([[0], np.cumsum(ns)])
+    A0 = pg.from_double_dev(torch.rand(int(offA[-1]), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    X = pg.from_double_dev(torch.rand(int(offB[-1]), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    for i in np.nonzero(kinds == pg.BATCH_CHOLESKY)[0]:
+        n = int(ns[i])
+        M = torch.rand(n, n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        S = (M @ M.t() / n + torch.eye(n, dtype=torch.float64, device=dev)).t().contiguous().reshape(-1)
+        A0[offA[i]:offA[i + 1]] = pg.from_double_dev(S)
+    B0 = torch.zeros_like(X)
+    view = lambda t, o, i: t[int(o[i]):int(o[i + 1])]
+    rhs_plan = pg.BatchGemmPlan([("N", "N", int(ns[i]), 1, int(ns[i]), pg.P32_ONE, view(A0, offA, i), int(ns[i]),
+                                  view(X, offB, i), int(ns[i]), 0, view(B0, offB, i), int(ns[i])) for i in range(P)])
+    rhs_plan.launch()  # b = A*x_true for every problem, batched (Rgemv 'N' bits)
+    A = A0.clone()
+    B = B0.clone()
+    ipiv = torch.zeros(int(offB[-1]), dtype=torch.int32, device=dev)
+    info = torch.zeros(P, dtype=torch.int32, device=dev)
+    plan = pg.BatchPlan([(int(kinds[i]), view(A, offA, i), view(B, offB, i), view(ipiv, offB, i), info[i:i + 1])
+                         for i in range(P)])
+    times = []
+    for r in range(args.warmup + args.steps):
+        A.copy_(A0)
+        B.copy_(B0)
+        e0, e1 = _events()
+        e0.record()
+        plan.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        if r >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    batch_ms = sum(times) / len(times)
+    # per-call path on a sample (same problems, same order)
+    S_ = min(P, 400)
+    Ac = A0.clone()
+    Bc = B0.clone()
+    ipc = torch.zeros_like(ipiv)
+    infc = torch.zeros_like(info)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for i in range(S_):
+        n = int(ns[i])
+        a, b_, ip = view(Ac, offA, i), view(Bc, offB, i), view(ipc, offB, i)
+        if kinds[i] == pg.BATCH_LU:
+            pg.Rgetrf_dev(n, n, a, n, ip, infc[i:i + 1])
+            pg.Rgetrs_dev("N", n, 1, a, n, ip, b_, n)
+        else:
+            pg.Rpotrf_dev("L", n, a, n, infc[i:i + 1])
+            pg.Rpotrs_dev("L", n, 1, a, n, b_, n)
+    e1.record()
+    torch.cuda.synchronize()
+    percall_ms = e0.elapsed_time(e1)
+    same = all(torch.equal(view(Ac, offA, i), view(A, offA, i)) and torch.equal(view(Bc, offB, i), view(B, offB, i))
+               for i in range(S_))
+    # GEMM batch
+    G = args.gemms
+    gm, gn, gk = _logu(rng, 4, 512, G), _logu(rng, 4, 512, G), _logu(rng, 4, 512, G)
+    ta = rng.choice(["N", "T"], G)
+    tb = rng.choice(["N", "T"], G)
+    oA = np.concatenate([[0], np.cumsum(gm * gk)])
+    oB = np.concatenate([[0], np.cumsum(gk * gn)])
+    oC = np.concatenate([[0], np.cumsum(gm * gn)])
+    GA = pg.from_double_dev(torch.rand(int(oA[-1]), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    GB = pg.from_double_dev(torch.rand(int(oB[-1]), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    GC0 = pg.from_double_dev(torch.rand(int(oC[-1]), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+    GC = GC0.clone()
+
+    def gprob(i, C):
+        m, n, k = int(gm[i]), int(gn[i]), int(gk[i])
+        return (ta[i], tb[i], m, n, k, pg.P32_MINUS_ONE, view(GA, oA, i), m if ta[i] == "N" else k,
+                view(GB, oB, i), k if tb[i] == "N" else n, pg.P32_ONE, view(C, oC, i), m)
+
+    gplan = pg.BatchGemmPlan([gprob(i, GC) for i in range(G)], tile_table=autotune.gemm_tile_table())
+    gt = []
+    for r in range(args.warmup + args.steps):
+        GC.copy_(GC0)
+        e0, e1 = _events()
+        e0.record()
+        gplan.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        if r >= args.warmup:
+            gt.append(e0.elapsed_time(e1))
+    gbatch_ms = sum(gt) / len(gt)
+    ops = float(np.sum(2.0 * gm * gn * gk))
+    GS = min(G, 2000)
+    GCc = GC0.clone()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for i in range(GS):
+        pg.Rgemm_dev(*gprob(i, GCc))
+    e1.record()
+    torch.cuda.synchronize()
+    gpercall_ms = e0.elapsed_time(e1)
+    gsame = all(torch.equal(view(GCc, oC, i), view(GC, oC, i)) for i in range(GS))
+    ops_s = float(np.sum(2.0 * gm[:GS] * gn[:GS] * gk[:GS]))
+    value = P / (batch_ms / 1e3)
+    line = {"metric": "batched posit32 LU/Cholesky factor+solve solves/s (20,000 problems, n log-uniform 8..512)",
+            "value": round(value, 1), "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(batch_ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "posit32", "data": "synthetic",
+            "config": {"workload": "config 4: 50% LU / 50% Cholesky(L), nrhs 1, b = A*x_true; "
+                                   "50,000 GEMMs m,n,k log-uniform 4..512, random transposes, alpha=-1, beta=1"},
+            "per_call_solves_per_s": round(S_ / (percall_ms / 1e3), 1), "per_call_sample": S_,
+            "speedup_vs_per_call": round(value / (S_ / (percall_ms / 1e3)), 2),
+            "bit_identical_to_per_call_on_sample": bool(same),
+            "gemm_batch": {"gemms": G, "ms": round(gbatch_ms, 3), "gop_s": round(ops / (gbatch_ms / 1e3) / 1e9, 2),
+                           "gemms_per_s": round(G / (gbatch_ms / 1e3), 1),
+                           "per_call_gop_s": round(ops_s / (gpercall_ms / 1e3) / 1e9, 2),
+                           "per_call_gemms_per_s": round(GS / (gpercall_ms / 1e3), 1), "per_call_sample": GS,
+                           "bit_identical_to_per_call_on_sample": bool(gsame),
+                           "tile_table": autotune.gemm_tile_table()},
+            "max_info": int(info.max().item())}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload in ("lu", "cholesky"):
+        return factor_arm(args)
+    if args.workload == "batch":
+        return batch_arm(args)
     return ours(args)
 
 

@@ -127,7 +127,28 @@ typedef struct posit_batch_plan posit_batch_plan;
 /* Uploads the descriptors (host array) and captures the launch; returns 0, 1/2 for bad
  * arguments / a bad descriptor, or POSIT_E_*. */
 int posit_batch_plan_create(const posit_batch_problem *probs, int nprob, posit_batch_plan **plan);
-/* Replays the captured launch on `stream` (asynchronous). */
+/* Many independent GEMMs (device pointers), each with the semantics and bits of
+ * posit_rgemm_dev, in ONE persistent kernel fed by a device queue of output tiles
+ * (longest k first), captured in a CUDA graph.  tile_table (9 ints, or NULL for the
+ * built-in default) maps the (m, n) size bucket -- row: m <= 32, <= 64, > 64; column: the
+ * same for n -- to a tile shape: 0 = 64x32, 1 = 32x32, 2 = 32x64 outputs per block; the
+ * autotuner (posit_gpu_b200/autotune.py) measures it.  A bad argument returns its Rgemm
+ * info code and its problem index in *bad_index. */
+typedef struct {
+    char transa, transb;
+    int m, n, k;
+    uint32_t alpha, beta;
+    const uint32_t *A;
+    int lda;
+    const uint32_t *B;
+    int ldb;
+    uint32_t *C;
+    int ldc;
+} posit_batch_gemm;
+int posit_batch_gemm_plan_create(const posit_batch_gemm *probs, int nprob, const int *tile_table,
+                                 posit_batch_plan **plan, int *bad_index);
+
+/* Replays a plan's captured launch on `stream` (asynchronous). */
 int posit_batch_plan_launch(posit_batch_plan *plan, void *stream);
 void posit_batch_plan_destroy(posit_batch_plan *plan);
 

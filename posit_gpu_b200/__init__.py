@@ -292,6 +292,44 @@ class BatchPlan:
             self._h = None
 
 
+class _BatchGemm(_c.Structure):
+    _fields_ = [("transa", _c.c_char), ("transb", _c.c_char), ("m", _c.c_int), ("n", _c.c_int), ("k", _c.c_int),
+                ("alpha", _c.c_uint32), ("beta", _c.c_uint32), ("A", _VP), ("lda", _c.c_int), ("B", _VP),
+                ("ldb", _c.c_int), ("C", _VP), ("ldc", _c.c_int)]
+
+
+_lib.posit_batch_gemm_plan_create.argtypes = [_c.POINTER(_BatchGemm), _c.c_int, _c.POINTER(_c.c_int),
+                                              _c.POINTER(_VP), _c.POINTER(_c.c_int)]
+_lib.posit_batch_gemm_plan_create.restype = _c.c_int
+
+
+class BatchGemmPlan(BatchPlan):
+    """Many independent Rgemm calls in one graph-captured persistent launch.
+
+    problems: iterable of (transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+    with A, B, C CUDA tensors of 4-byte posit patterns (kept alive by the plan).
+    tile_table: 9 ints (size bucket -> tile shape), default: the built-in table."""
+
+    def __init__(self, problems, tile_table=None):
+        probs = list(problems)
+        arr = (_BatchGemm * max(1, len(probs)))()
+        self._keep = []
+        for i, (ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc) in enumerate(probs):
+            arr[i] = _BatchGemm(_char(ta), _char(tb), m, n, k, int(alpha) & 0xFFFFFFFF, int(beta) & 0xFFFFFFFF,
+                                A.data_ptr(), lda, B.data_ptr(), ldb, C.data_ptr(), ldc)
+            self._keep.append((A, B, C))
+        tt = None
+        if tile_table is not None:
+            tt = (_c.c_int * 9)(*[int(x) for x in tile_table])
+        h, bad = _VP(), _c.c_int(-1)
+        rc = _lib.posit_batch_gemm_plan_create(arr, len(probs), tt, _c.byref(h), _c.byref(bad))
+        if rc > 0:
+            raise ValueError(f" ** On entry to Rgemm  parameter number {rc:2d} had an illegal value "
+                             f"(batch problem {bad.value})")
+        _check(rc, "batch gemm plan")
+        self._h = h
+
+
 NOALLOC_SCRATCH_BYTES = 64 << 20
 POSIT_E_NOALLOC_LIMIT = -6
 

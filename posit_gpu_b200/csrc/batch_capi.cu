@@ -1,6 +1,9 @@
 // batch_capi.cu -- C ABI for batched factor-and-solve plans (include/posit_gpu.h).
 #include "../../include/posit_gpu.h"
 #include "batch.cuh"
+#include "batch_gemm.cuh"
+
+#include <ctype.h>
 
 #include <algorithm>
 #include <new>
@@ -10,8 +13,8 @@
 struct posit_batch_plan {
     int nprob = 0;
     int ctas = 0;
-    pg::BatchProblem *d_probs = nullptr;
-    int *d_order = nullptr;
+    void *d_probs = nullptr; // pg::BatchProblem[] or pg::BatchGemmDesc[]
+    void *d_order = nullptr; // int[] (factor plans) or pg::BatchTile[] (GEMM plans)
     int *d_next = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -55,7 +58,7 @@ extern "C" int posit_batch_plan_create(const posit_batch_problem *probs, int npr
     std::vector<int> order(nprob);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return probs[a].n > probs[b].n; });
-    cudaError_t e = cudaMalloc(&p->d_probs, sizeof(pg::BatchProblem) * (nprob > 0 ? nprob : 1));
+    cudaError_t e = cudaMalloc((void **)&p->d_probs, sizeof(pg::BatchProblem) * (nprob > 0 ? nprob : 1));
     if (e == cudaSuccess)
         e = cudaMalloc(&p->d_order, sizeof(int) * (nprob > 0 ? nprob : 1));
     if (e == cudaSuccess)
@@ -71,7 +74,130 @@ extern "C" int posit_batch_plan_create(const posit_batch_problem *probs, int npr
     if (e == cudaSuccess) {
         e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            cudaError_t le = pg::batch_factor_launch(p->d_probs, nprob, p->d_order, p->d_next, p->ctas, cs);
+            cudaError_t le = pg::batch_factor_launch(reinterpret_cast<pg::BatchProblem *>(p->d_probs), nprob,
+                                                     reinterpret_cast<int *>(p->d_order), p->d_next, p->ctas, cs);
+            e = cudaStreamEndCapture(cs, &p->graph);
+            if (e == cudaSuccess)
+                e = le;
+        }
+        cudaStreamDestroy(cs);
+    }
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    if (e != cudaSuccess) {
+        plan_free(p);
+        return e == cudaErrorMemoryAllocation ? POSIT_E_NO_MEMORY : POSIT_E_CUDA;
+    }
+    *out = p;
+    return 0;
+}
+
+// ---- batched GEMM -------------------------------------------------------------
+static bool same_c(char a, char b) { return toupper((unsigned char)a) == toupper((unsigned char)b); }
+
+// Rgemm.cpp:90-128 checks for one problem.
+static int gemm_args(const posit_batch_gemm &q)
+{
+    bool nota = same_c(q.transa, 'N'), notb = same_c(q.transb, 'N');
+    int nrowa = nota ? q.m : q.k, nrowb = notb ? q.k : q.n;
+    if (!nota && !same_c(q.transa, 'C') && !same_c(q.transa, 'T'))
+        return 1;
+    if (!notb && !same_c(q.transb, 'C') && !same_c(q.transb, 'T'))
+        return 2;
+    if (q.m < 0)
+        return 3;
+    if (q.n < 0)
+        return 4;
+    if (q.k < 0)
+        return 5;
+    if (q.lda < (nrowa > 1 ? nrowa : 1))
+        return 8;
+    if (q.ldb < (nrowb > 1 ? nrowb : 1))
+        return 10;
+    if (q.ldc < (q.m > 1 ? q.m : 1))
+        return 13;
+    return 0;
+}
+
+static int size_bucket(int x) { return x <= 32 ? 0 : (x <= 64 ? 1 : 2); }
+
+// Default tile-shape table (rows: m bucket <=32, <=64, >64; columns: n bucket), used
+// when the caller passes none: 32x32 for small problems, 32x64 for short-and-wide ones,
+// 64x32 otherwise.
+static const int kDefaultTileTable[9] = {1, 2, 2, 0, 0, 0, 0, 0, 0};
+
+extern "C" int posit_batch_gemm_plan_create(const posit_batch_gemm *probs, int nprob, const int *tile_table,
+                                            posit_batch_plan **out, int *bad_index)
+{
+    if (!probs || nprob < 0 || !out)
+        return POSIT_E_WORKSPACE;
+    const int *table = tile_table ? tile_table : kDefaultTileTable;
+    for (int c = 0; c < 9; ++c)
+        if (table[c] < 0 || table[c] >= pg::BATCH_TILE_CONFIGS)
+            return POSIT_E_WORKSPACE;
+    std::vector<pg::BatchGemmDesc> desc(nprob > 0 ? nprob : 1);
+    std::vector<pg::BatchTile> tiles;
+    for (int i = 0; i < nprob; ++i) {
+        const posit_batch_gemm &q = probs[i];
+        int info = gemm_args(q);
+        if (info) {
+            if (bad_index)
+                *bad_index = i;
+            return info;
+        }
+        pg::BatchGemmDesc &d = desc[i];
+        d.nota = same_c(q.transa, 'N');
+        d.notb = same_c(q.transb, 'N');
+        d.m = q.m;
+        d.n = q.n;
+        d.k = q.k;
+        d.alpha = q.alpha;
+        d.beta = q.beta;
+        d.A = q.A;
+        d.lda = q.lda;
+        d.B = q.B;
+        d.ldb = q.ldb;
+        d.C = q.C;
+        d.ldc = q.ldc;
+        // quick return (Rgemm.cpp:134-136): no work at all
+        if (q.m == 0 || q.n == 0 || ((q.alpha == 0 || q.k == 0) && q.beta == 0x40000000u))
+            continue;
+        const int cfg = table[size_bucket(q.m) * 3 + size_bucket(q.n)];
+        const int bm = pg::batch_tile_rows(cfg), bn = pg::batch_tile_cols(cfg);
+        for (int nt = 0; nt < (q.n + bn - 1) / bn; ++nt)
+            for (int mt = 0; mt < (q.m + bm - 1) / bm; ++mt)
+                tiles.push_back(pg::BatchTile{i, mt, nt, cfg});
+    }
+    // longest k first
+    std::stable_sort(tiles.begin(), tiles.end(),
+                     [&](const pg::BatchTile &a, const pg::BatchTile &b) { return desc[a.prob].k > desc[b.prob].k; });
+    posit_batch_plan *p = new (std::nothrow) posit_batch_plan();
+    if (!p)
+        return POSIT_E_NO_MEMORY;
+    p->nprob = (int)tiles.size();
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    p->ctas = sms * 2;
+    const size_t nt = tiles.size() > 0 ? tiles.size() : 1;
+    cudaError_t e = cudaMalloc(&p->d_probs, sizeof(pg::BatchGemmDesc) * desc.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&p->d_order, sizeof(pg::BatchTile) * nt);
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&p->d_next, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->d_probs, desc.data(), sizeof(pg::BatchGemmDesc) * desc.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !tiles.empty())
+        e = cudaMemcpy(p->d_order, tiles.data(), sizeof(pg::BatchTile) * tiles.size(), cudaMemcpyHostToDevice);
+    cudaStream_t cs = nullptr;
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t le = pg::batch_gemm_launch(reinterpret_cast<pg::BatchGemmDesc *>(p->d_probs),
+                                                   reinterpret_cast<pg::BatchTile *>(p->d_order), p->nprob,
+                                                   p->d_next, p->ctas, cs);
             e = cudaStreamEndCapture(cs, &p->graph);
             if (e == cudaSuccess)
                 e = le;

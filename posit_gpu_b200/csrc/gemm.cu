@@ -22,6 +22,7 @@
 //     integer-only and branch-free; the rare step that leaves the fast range (long
 //     regimes, zero or NaR operands, exact cancellation) is redone exactly afterwards.
 #include "gemm.cuh"
+#include "gemm_tile.cuh"
 #include "posit32.cuh"
 
 #include <mutex>
@@ -82,23 +83,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
-}
-
-// ---------------------------------------------------------------------------
-// Decoded element packing: {scale, significand | sign << 31}
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint2 pack_dp(const dp32 &d)
-{
-    return make_uint2((uint32_t)d.s, d.g | (d.x << 31));
-}
-
-__device__ __forceinline__ dp32 unpack_dp(uint32_t s, uint32_t gx)
-{
-    dp32 d;
-    d.s = (int32_t)s;
-    d.g = gx & 0x7FFFFFFFu;
-    d.x = gx >> 31;
-    return d;
 }
 
 GemmPlan gemm_plan(int m, int n, int k)
@@ -184,10 +168,6 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
 // ---------------------------------------------------------------------------
 // Main kernel
 // ---------------------------------------------------------------------------
-// Thread (tx, ty) owns rows {2tx, 2tx+1, 32+2tx, 33+2tx} and the same pattern of
-// columns with ty: the 16-byte shared-memory loads of a warp then hit distinct banks.
-__device__ __forceinline__ int own_off(int t, int q) { return (q >> 1) * 32 + 2 * t + (q & 1); }
-
 // LOWER: only entries with row >= column are written (tiles wholly above the diagonal
 // exit at once) -- the symmetric trailing update of a lower Cholesky factorization.
 // `stop`, if given, is a device flag (a factorization's info) that turns the call into a
@@ -272,47 +252,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
         const uint2 *as = As + s * BK * BM;
         const uint2 *ts = Ts + s * BK * BN;
         const int lmax = min(BK, k - kt * BK);
-        for (int l = 0; l < lmax; ++l) {
-            dp32 a[TM], t[TN];
-#pragma unroll
-            for (int q = 0; q < TM / 2; ++q) {
-                const uint4 v = *reinterpret_cast<const uint4 *>(as + l * BM + 32 * q + 2 * tx);
-                a[2 * q] = unpack_dp(v.x, v.y);
-                a[2 * q + 1] = unpack_dp(v.z, v.w);
-            }
-#pragma unroll
-            for (int q = 0; q < TN / 2; ++q) {
-                const uint4 v = *reinterpret_cast<const uint4 *>(ts + l * BN + 32 * q + 2 * ty);
-                t[2 * q] = unpack_dp(v.x, v.y);
-                t[2 * q + 1] = unpack_dp(v.z, v.w);
-            }
-            uint32_t fail = 0;
-#pragma unroll
-            for (int i = 0; i < TM; ++i) {
-#pragma unroll
-                for (int j = 0; j < TN; ++j) {
-                    dp32 p, r;
-                    uint32_t bm, ba;
-                    dmul_fast(t[j], a[i], tbl, p, bm);
-                    dadd_fast(acc[i][j], p, tbl, r, ba);
-                    // branch-free commit: a failed step leaves the accumulator as it was,
-                    // and sets bit i*TN+j of `fail` (umulhi(2^30, 2^(idx+2)) = 2^idx)
-                    const uint32_t v = (bm | ba) & 0x40000000u;
-                    acc[i][j].s = v ? acc[i][j].s : r.s;
-                    acc[i][j].g = v ? acc[i][j].g : r.g;
-                    acc[i][j].x = v ? acc[i][j].x : r.x;
-                    fail += __umulhi(v, 4u << (i * TN + j));
-                }
-            }
-            if (fail) { // rare: redo the failed steps exactly, in the same order
-#pragma unroll
-                for (int i = 0; i < TM; ++i)
-#pragma unroll
-                    for (int j = 0; j < TN; ++j)
-                        if (fail & (1u << (i * TN + j)))
-                            acc[i][j] = dmac_exact(acc[i][j], t[j], a[i]);
-            }
-        }
+        tile_steps<TM, TN>(acc, as, ts, lmax, tbl, tx, ty);
         // every thread is done with stage s before it is refilled
         bad = __syncthreads_or(!arrived) != 0;
         if (bad)
