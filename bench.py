@@ -52,12 +52,16 @@ def parse():
     ap.add_argument("--trans", default="NN")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="gemm", choices=["gemm", "lu", "cholesky", "batch"],
+    ap.add_argument("--workload", default="gemm", choices=["gemm", "lu", "cholesky", "batch", "serve"],
                     help="gemm (default, the headline), lu / cholesky (device-resident "
                          "factorization + solve, FP64 errors), batch (batched vs per-call)")
     ap.add_argument("--nb", type=int, default=0, help="panel width for lu/cholesky (0: tuned)")
     ap.add_argument("--problems", type=int, default=20000, help="batch: factor-and-solve problems")
     ap.add_argument("--gemms", type=int, default=50000, help="batch: GEMM problems")
+    ap.add_argument("--requests", type=int, default=300, help="serve: requests per arrival rate")
+    ap.add_argument("--rates", default="5,10,20,40,burst", help="serve: Poisson arrival rates (req/s)")
+    ap.add_argument("--per-call-sample", type=int, default=100, help="serve: requests timed on the per-call path")
+    ap.add_argument("--batch-max-n", type=int, default=0, help="serve: batched-kernel size limit (0: default)")
     return ap.parse_args()
 
 
@@ -558,6 +562,184 @@ def batch_arm(args):
     return 0
 
 
+def _serve_workload(R, seed=5150):
+    """Configuration 5's request stream: LU / Cholesky 50/50, n log-uniform 32..4096,
+    nrhs uniform 1..16, 30% of requests reusing an earlier request's matrix (kind and n
+    included) with new right-hand sides.  Returns per-request (kind, n, nrhs, matrix id)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    kinds = np.where(rng.random(R) < 0.5, 0, 1)
+    ns = _logu(rng, 32, 4096, R)
+    nrhs = rng.integers(1, 17, R)
+    mid = np.arange(R)
+    for i in range(1, R):
+        if rng.random() < 0.3:
+            j = int(rng.integers(0, i))
+            mid[i], kinds[i], ns[i] = mid[j], kinds[j], ns[j]
+    return [(int(kinds[i]), int(ns[i]), int(nrhs[i]), int(mid[i])) for i in range(R)]
+
+
+def _serve_data(reqs):
+    """Matrices (config 3's distributions: U[-1,1] for LU, M*M^T/n + I for Cholesky) seeded
+    per matrix, right-hand sides B = A*X_true (FP64 of the posit values, X_true ~ U[-1,1])
+    seeded per request; everything lands in page-locked host buffers."""
+    import torch
+
+    import posit_gpu_b200 as pg
+    dev = torch.device("cuda")
+    f64 = torch.float64
+    mats, rhs = {}, []
+    for i, (kind, n, r, m) in enumerate(reqs):
+        g = torch.Generator(device=dev)
+        if m not in mats:
+            g.manual_seed(1_000_003 * m + 17)
+            if kind == 0:
+                Ad = pg.from_double_dev(torch.rand(n * n, dtype=f64, device=dev, generator=g) * 2 - 1)
+            else:
+                M = torch.rand(n, n, dtype=f64, device=dev, generator=g) * 2 - 1
+                Ad = pg.from_double_dev((M @ M.t() / n + torch.eye(n, dtype=f64, device=dev)).reshape(-1))
+                del M
+            host = torch.empty(n * n, dtype=torch.int32, pin_memory=True)
+            host.copy_(Ad)
+            mats[m] = host
+        g.manual_seed(7_000_001 * i + 5)
+        A64 = pg.to_double_dev(mats[m].to(dev)).reshape(n, n).t()  # column-major
+        X64 = pg.to_double_dev(pg.from_double_dev(torch.rand(n * r, dtype=f64, device=dev, generator=g) * 2 - 1))
+        B64 = A64 @ X64.reshape(r, n).t()
+        Bh = torch.empty(n * r, dtype=torch.int32, pin_memory=True)
+        Bh.copy_(pg.from_double_dev(B64.t().contiguous().reshape(-1)))
+        rhs.append(Bh)
+    torch.cuda.synchronize()
+    return mats, rhs
+
+
+def _percentile(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs), q)) if len(xs) else None
+
+
+def serve_arm(args):
+    """Configuration 5: served Ax = b requests at Poisson arrival rates (and a burst),
+    through the library's request loop (posit_server_*): continuous admission under the
+    150 GB device budget, batched small systems, blocked large ones overlapping on the GPU,
+    factors cached on the device for repeat matrices.  Against the plain per-call drop-in
+    path (posit_rgetrf + posit_rgetrs / posit_rpotrf + posit_rpotrs on host buffers, one
+    request after another, reusing host-side factors for repeat matrices) on a sample of
+    the same stream.  Every served solution is compared bit for bit with the per-call one
+    and across rates.  Times are host wall-clock from submit to the solution in host
+    memory (end to end: H2D of A and B, D2H of X inside)."""
+    import numpy as np
+    import torch
+
+    import posit_gpu_b200 as pg
+    R = args.requests
+    reqs = _serve_workload(R)
+    mats, rhs = _serve_data(reqs)
+    zeros = lambda i: torch.zeros(reqs[i][1] * reqs[i][2], dtype=torch.int32, pin_memory=True)
+
+    # plain per-call path, one request after another
+    S = min(R, args.per_call_sample)
+    fac_src = {m: mats[m].numpy().view(np.uint32).copy() for (_, _, _, m) in reqs[:S]}
+    xs = [rhs[i].numpy().view(np.uint32).copy() for i in range(S)]
+    pc_info, factors, pc_lat = [], {}, []
+    t0 = time.perf_counter()
+    for i in range(S):
+        kind, n, r, m = reqs[i]
+        ts = time.perf_counter()
+        if m not in factors:
+            F = fac_src[m]
+            ipiv = np.zeros(n, np.int32)
+            info = pg.Rgetrf(n, n, F, n, ipiv, nb=64) if kind == 0 else pg.Rpotrf("L", n, F, n, nb=64)
+            factors[m] = (F, ipiv, info)
+        F, ipiv, info = factors[m]
+        if kind == 0:
+            pg.Rgetrs("N", n, r, F, n, ipiv, xs[i], n)
+        elif info == 0:
+            pg.Rpotrs("L", n, r, F, n, xs[i], n)
+        pc_info.append(info)
+        pc_lat.append((time.perf_counter() - ts) * 1e3)
+    pc_s = time.perf_counter() - t0
+    pc_rate = S / pc_s
+
+    # served, at each arrival rate
+    rates = [r.strip() for r in args.rates.split(",") if r.strip()]
+    runs, served_x, clocks = [], None, None
+    same_across = True
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    for rate in rates:
+        outs = [zeros(i) for i in range(R)]
+        arng = np.random.default_rng(77)
+        gaps = np.zeros(R) if rate == "burst" else arng.exponential(1.0 / float(rate), R)
+        arrive = np.cumsum(gaps) - gaps[0]
+        with pg.Server(batch_max_n=args.batch_max_n) as srv:
+            tickets, t_sub = [None] * R, [0.0] * R
+
+            def feed():
+                base = time.perf_counter()
+                for i, (kind, n, r, m) in enumerate(reqs):
+                    delay = base + arrive[i] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    t_sub[i] = time.perf_counter()
+                    tickets[i] = srv.submit(kind, n, r, mats[m], rhs[i], outs[i], matrix_id=m)
+
+            th = threading.Thread(target=feed)
+            th.start()
+            th.join()
+            res = [srv.wait(t) for t in tickets]
+            st = srv.stats()
+        lat = [x["latency_ms"] for x in res]
+        span = max(t_sub[i] + lat[i] / 1e3 for i in range(R)) - t_sub[0]
+        ok = all(x["status"] == 0 for x in res)
+        hits = sum(x["cache_hit"] for x in res)
+        xs_run = [o.numpy().view(np.uint32) for o in outs]
+        same_pc = all(res[i]["info"] == pc_info[i] and (pc_info[i] != 0 or np.array_equal(xs_run[i], xs[i]))
+                      for i in range(S))
+        if served_x is None:
+            served_x = (xs_run, [x["info"] for x in res])
+        else:
+            same_across &= all(served_x[1][i] == res[i]["info"] and
+                               (res[i]["info"] != 0 or np.array_equal(served_x[0][i], xs_run[i])) for i in range(R))
+        by_path = {p: [x["latency_ms"] for x in res if x["path"] == p] for p in (0, 1)}
+        slow = sorted(range(R), key=lambda i: -lat[i])[:4]
+        slowest = [{"kind": "LU" if reqs[i][0] == 0 else "Cholesky", "n": reqs[i][1], "nrhs": reqs[i][2],
+                    "path": res[i]["path"], "hit": res[i]["cache_hit"], "ms": round(lat[i], 1),
+                    "queue_ms": round(res[i]["queue_ms"], 1)} for i in slow]
+        runs.append({"rate_req_s": rate, "solves_per_s": round(R / span, 2),
+                     "rhs_per_s": round(sum(q[2] for q in reqs) / span, 1),
+                     "p50_ms": round(_percentile(lat, 50), 2), "p99_ms": round(_percentile(lat, 99), 2),
+                     "p50_queue_ms": round(_percentile([x["queue_ms"] for x in res], 50), 3),
+                     "p99_batched_ms": round(_percentile(by_path[0], 99) or 0, 2),
+                     "p99_blocked_ms": round(_percentile(by_path[1], 99) or 0, 2),
+                     "all_ok": ok, "cache_hits": hits, "inflight_peak": st["inflight_peak"],
+                     "batched_units": st["batched_units"], "blocked_units": st["blocked_units"],
+                     "evictions": st["evictions"], "bytes_peak_gb": round(st["bytes_peak"] / 1e9, 2),
+                     "bit_identical_to_per_call_on_sample": bool(same_pc), "slowest": slowest})
+    clocks = sampler.stop()
+    repeats = sum(1 for i, q in enumerate(reqs) if q[3] != i)
+    best = max(runs, key=lambda x: x["solves_per_s"])
+    h2d = sum(4 * (q[1] * q[1] + q[1] * q[2]) for q in reqs) / R
+    line = {"metric": "served posit32 Ax=b solves/s (LU/Cholesky, n log-uniform 32..4096, nrhs 1..16), "
+                      "p50/p99 latency, bit-identical to per-call",
+            "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(rates), "warmup": 0,
+            "ms_per_step": round(1e3 / best["solves_per_s"], 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "posit32", "data": "synthetic",
+            "config": {"workload": f"config 5: {R} requests, 50% LU / 50% Cholesky(L), {repeats} repeat "
+                                   "matrices (30%), B = A*X_true, Poisson arrivals per rate, 150 GB budget",
+                       "rates": rates, "batch_max_n": args.batch_max_n or 256},
+            "e2e": {"value": best["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": round(h2d),
+                    "d2h_bytes_per_step": round(sum(4 * q[1] * q[2] for q in reqs) / R),
+                    "note": "value is itself end to end: host buffers in, solution in host memory"},
+            "rates": runs, "per_call": {"solves_per_s": round(pc_rate, 2), "sample": S,
+                                        "p50_ms": round(_percentile(pc_lat, 50), 2),
+                                        "p99_ms": round(_percentile(pc_lat, 99), 2)},
+            "speedup_vs_per_call": round(best["solves_per_s"] / pc_rate, 2),
+            "bit_identical_across_rates": bool(same_across), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -566,6 +748,8 @@ def main():
         return factor_arm(args)
     if args.workload == "batch":
         return batch_arm(args)
+    if args.workload == "serve":
+        return serve_arm(args)
     return ours(args)
 
 

@@ -91,17 +91,17 @@ size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
  * synchronous.  Only trans = 'N' (Rgetrs) and uplo = 'L' (Rpotrf/Rpotrs) run on the
  * device; the others return POSIT_E_UNSUPPORTED. */
 
-/* Rgetrf (libRpack/Rgetrf.cpp:32-137; mplapack_posit.h:104), Rgetrf_opencl (mplapack_posit.h:105) */
+/* Rgetrf (libRpack/Rgetrf.cpp:32-137; mplapack_posit.h:48), Rgetrf_opencl (mplapack_posit.h:49) */
 int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream);
 int posit_rgetrf(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info);
-/* Rgetrs (libRpack/Rgetrs.cpp:32-118; mplapack_posit.h:102) */
+/* Rgetrs (libRpack/Rgetrs.cpp:32-118; mplapack_posit.h:46) */
 int posit_rgetrs_dev(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B,
                      int ldb, void *stream);
 int posit_rgetrs(char trans, int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb);
-/* Rpotrf (libRpack/Rpotrf.cpp:32-154; mplapack_posit.h:94), Rpotrf_opencl (mplapack_posit.h:99) */
+/* Rpotrf (libRpack/Rpotrf.cpp:32-154; mplapack_posit.h:38), Rpotrf_opencl (mplapack_posit.h:43) */
 int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, void *stream);
 int posit_rpotrf(char uplo, int n, uint32_t *A, int lda, int nb, int *info);
-/* Rpotrs (libRpack/Rpotrs.cpp:32-110; mplapack_posit.h:97) */
+/* Rpotrs (libRpack/Rpotrs.cpp:32-110; mplapack_posit.h:41) */
 int posit_rpotrs_dev(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, void *stream);
 int posit_rpotrs(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb);
 
@@ -151,6 +151,80 @@ int posit_batch_gemm_plan_create(const posit_batch_gemm *probs, int nprob, const
 /* Replays a plan's captured launch on `stream` (asynchronous). */
 int posit_batch_plan_launch(posit_batch_plan *plan, void *stream);
 void posit_batch_plan_destroy(posit_batch_plan *plan);
+
+/* ---- Served solves (no reference counterpart) ---------------------------------------
+ * A request loop for Ax = b solves of mixed kind, n and nrhs that arrive over time.  A
+ * loop thread admits queued requests in arrival order while admitted-but-unfinished
+ * requests stay under max_inflight and their device bytes (matrix/factor, right-hand
+ * sides, workspace) under the memory budget, evicting idle cached factors (least
+ * recently used first) when it is short; a request that finds no free lane of its kind
+ * waits, and so do later ones of that kind, while the other kind moves on.  Requests with n <= batch_max_n admitted
+ * together run as one launch of the batched kernel above; larger ones run the blocked
+ * device path (posit_rgetrf_dev + posit_rgetrs_dev, posit_rpotrf_dev('L') +
+ * posit_rpotrs_dev('L')), each on a stream of its own, so units overlap on the GPU and
+ * requests that arrive meanwhile are admitted as lanes, slots and memory free up.  A
+ * request with matrix_id >= 0 leaves its factor on the device; a later request with the
+ * same id runs the solve only (its A may then be NULL).
+ *
+ * Results are bit-identical to the per-call path -- and so to the CPU Rgetrf/Rgetrs,
+ * Rpotrf/Rpotrs -- whether served alone, in any mix, or from the cache.  When info != 0
+ * the contents of X are unspecified.  Host buffers must stay valid until the request is
+ * finished; page-locked buffers are copied asynchronously, pageable ones cost a host copy
+ * on the serving threads.  Multiple client threads may submit and wait concurrently. */
+#define POSIT_E_QUEUE_FULL (-8)      /* the server's queue holds max_queue requests */
+#define POSIT_E_CANCELLED (-9)       /* cancelled before admission, or the server shut down */
+#define POSIT_E_NOT_CACHED (-10)     /* A == NULL and no factor is cached under matrix_id */
+#define POSIT_E_MISMATCH (-11)       /* matrix_id cached with another kind or n */
+#define POSIT_E_UNKNOWN_TICKET (-12) /* no such ticket (or its result was already taken) */
+#define POSIT_SERVER_DEFAULT_BUDGET ((size_t)150000000000ull) /* 150 GB */
+typedef struct posit_server posit_server;
+typedef struct {
+    size_t memory_budget; /* device bytes; 0 = 150 GB (capped at free memory - 2 GiB) */
+    int max_inflight;     /* admitted, unfinished requests; 0 = 4096 */
+    int max_queue;        /* submitted, not yet admitted requests; 0 = 2^20 */
+    int lanes;            /* CUDA streams work units run on; 0 = 32 */
+    int launch_threads;   /* threads issuing the units' CUDA work; 0 = 4 */
+    int batch_max_n;      /* n <= this goes to the batched kernel; 0 = 256 (max POSIT_BATCH_MAX_N) */
+    int nb;               /* panel width of the blocked path; 0 = 64 */
+    int cache_off;        /* 1: never keep factors */
+    int batch_lanes;      /* lanes reserved for batched units; 0 = 4 */
+} posit_server_config;
+typedef struct {
+    int kind;             /* POSIT_BATCH_LU or POSIT_BATCH_CHOLESKY (lower) */
+    int n, nrhs;
+    long long matrix_id;  /* >= 0: cache the factor under this id (or use the cached one) */
+    const uint32_t *A;    /* host n x n, column-major, lda = n; NULL = use the cached factor */
+    const uint32_t *B;    /* host n x nrhs, ldb = n */
+    uint32_t *X;          /* host n x nrhs, receives the solution (may be B) */
+} posit_solve_request;
+typedef struct {
+    int status;           /* 0 or POSIT_E_* (the request did not run, or failed) */
+    int info;             /* the factorization's info (Rgetrf / Rpotrf) */
+    int cache_hit;        /* 1: solved on a cached factor */
+    int path;             /* 0: batched kernel, 1: blocked path */
+    double queue_ms;      /* submit -> admission */
+    double latency_ms;    /* submit -> solution in X */
+} posit_solve_result;
+typedef struct {
+    long long submitted, completed, failed, cancelled;
+    long long cache_hits, cache_misses, evictions;
+    long long batched_units, blocked_units, inflight_peak;
+    size_t budget_bytes, bytes_in_use, bytes_peak, cached_bytes;
+} posit_server_stats;
+/* 0 or POSIT_E_*; with cfg == NULL every field takes its default. */
+int posit_server_create(const posit_server_config *cfg, posit_server **server);
+/* Queues a request: 0 and a ticket, 1..6 for a bad argument (kind, n, nrhs, A, B, X), or
+ * POSIT_E_NO_MEMORY (can never fit the budget) / POSIT_E_QUEUE_FULL / POSIT_E_CANCELLED. */
+int posit_server_submit(posit_server *s, const posit_solve_request *req, long long *ticket);
+/* Blocks until the request is finished and takes its result (the ticket is then gone). */
+int posit_server_wait(posit_server *s, long long ticket, posit_solve_result *res);
+/* 1 and the result if finished (the ticket is then gone), 0 if not yet. */
+int posit_server_poll(posit_server *s, long long ticket, posit_solve_result *res);
+/* 0: cancelled (it had not been admitted); 1: admitted or finished already. */
+int posit_server_cancel(posit_server *s, long long ticket);
+int posit_server_get_stats(posit_server *s, posit_server_stats *st);
+/* Cancels queued requests, waits for admitted ones, frees everything. */
+void posit_server_destroy(posit_server *s);
 
 /* Element-wise conversions on device buffers, asynchronous on `stream`.
  * Replace the SoftPosit class conversions the reference drivers use to build their

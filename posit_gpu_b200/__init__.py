@@ -173,7 +173,7 @@ def to_double_dev(u, out=None, stream=None):
 
 
 # ---------------------------------------------------------------------------
-# LAPACK (libRpack/mplapack_posit.h:94-108): LU and Cholesky, bit-identical to the CPU
+# LAPACK (libRpack/mplapack_posit.h:38-52): LU and Cholesky, bit-identical to the CPU
 # routines.  Host forms take numpy buffers (4-byte elements; ipiv int32) and return the
 # reference's `info`; _dev forms take torch CUDA tensors and leave info on the device.
 # ---------------------------------------------------------------------------
@@ -364,3 +364,138 @@ def profile_read(reset=True):
     ms, mains, alls = _c.c_double(), _c.c_longlong(), _c.c_longlong()
     _lib.posit_profile_read(_c.byref(ms), _c.byref(mains), _c.byref(alls), 1 if reset else 0)
     return ms.value, mains.value, alls.value
+
+
+# ---------------------------------------------------------------------------
+# Served solves (no reference counterpart): include/posit_gpu.h, posit_server_*
+# ---------------------------------------------------------------------------
+class _ServerConfig(_c.Structure):
+    _fields_ = [("memory_budget", _c.c_size_t), ("max_inflight", _c.c_int), ("max_queue", _c.c_int),
+                ("lanes", _c.c_int), ("launch_threads", _c.c_int), ("batch_max_n", _c.c_int), ("nb", _c.c_int),
+                ("cache_off", _c.c_int), ("batch_lanes", _c.c_int)]
+
+
+class _SolveRequest(_c.Structure):
+    _fields_ = [("kind", _c.c_int), ("n", _c.c_int), ("nrhs", _c.c_int), ("matrix_id", _c.c_longlong),
+                ("A", _VP), ("B", _VP), ("X", _VP)]
+
+
+class _SolveResult(_c.Structure):
+    _fields_ = [("status", _c.c_int), ("info", _c.c_int), ("cache_hit", _c.c_int), ("path", _c.c_int),
+                ("queue_ms", _c.c_double), ("latency_ms", _c.c_double)]
+
+
+class _ServerStats(_c.Structure):
+    _fields_ = [(f, _c.c_longlong) for f in ("submitted", "completed", "failed", "cancelled", "cache_hits",
+                                            "cache_misses", "evictions", "batched_units", "blocked_units",
+                                            "inflight_peak")] + \
+               [(f, _c.c_size_t) for f in ("budget_bytes", "bytes_in_use", "bytes_peak", "cached_bytes")]
+
+
+_lib.posit_server_create.argtypes = [_c.POINTER(_ServerConfig), _c.POINTER(_VP)]
+_lib.posit_server_submit.argtypes = [_VP, _c.POINTER(_SolveRequest), _c.POINTER(_c.c_longlong)]
+_lib.posit_server_wait.argtypes = [_VP, _c.c_longlong, _c.POINTER(_SolveResult)]
+_lib.posit_server_poll.argtypes = [_VP, _c.c_longlong, _c.POINTER(_SolveResult)]
+_lib.posit_server_cancel.argtypes = [_VP, _c.c_longlong]
+_lib.posit_server_get_stats.argtypes = [_VP, _c.POINTER(_ServerStats)]
+_lib.posit_server_destroy.argtypes = [_VP]
+for _f in ("posit_server_create", "posit_server_submit", "posit_server_wait", "posit_server_poll",
+           "posit_server_cancel", "posit_server_get_stats"):
+    getattr(_lib, _f).restype = _I
+
+SOLVE_LU = BATCH_LU
+SOLVE_CHOLESKY = BATCH_CHOLESKY
+E_QUEUE_FULL, E_CANCELLED, E_NOT_CACHED, E_MISMATCH, E_UNKNOWN_TICKET = -8, -9, -10, -11, -12
+
+
+def _buf_ptr(x):
+    """Host buffer of 4-byte posit patterns: a numpy array or a CPU torch tensor
+    (page-locked ones are copied asynchronously)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return _host_ptr(x)
+    if getattr(x, "is_cuda", False) or not hasattr(x, "data_ptr"):
+        raise TypeError("served requests take host buffers (numpy arrays or CPU tensors)")
+    if x.element_size() != 4 or not x.is_contiguous():
+        raise TypeError("posit32 buffers hold 4-byte elements, contiguous")
+    return x.data_ptr()
+
+
+class Server:
+    """Served Ax = b solves: continuous admission under a device-memory budget, batched
+    small problems, blocked large ones overlapping on the GPU, and an on-device factor
+    cache keyed by matrix id.  Every solution is bit-identical to the per-call path.
+
+        srv = Server(memory_budget=150e9)
+        t = srv.submit(SOLVE_LU, n, nrhs, A, B, X, matrix_id=7)   # host buffers
+        res = srv.wait(t)     # {'status', 'info', 'cache_hit', 'path', 'queue_ms', 'latency_ms'}
+    """
+
+    def __init__(self, memory_budget=0, max_inflight=0, max_queue=0, lanes=0, launch_threads=0,
+                 batch_max_n=0, nb=0, cache=True, batch_lanes=0):
+        cfg = _ServerConfig(int(memory_budget), max_inflight, max_queue, lanes, launch_threads, batch_max_n, nb,
+                            0 if cache else 1, batch_lanes)
+        h = _VP()
+        _check(_lib.posit_server_create(_c.byref(cfg), _c.byref(h)), "server")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, kind, n, nrhs, A, B, X, matrix_id=-1):
+        """Queue one request (host buffers, column-major, lda = ldb = n); returns a ticket.
+        A may be None when matrix_id names a cached factor."""
+        q = _SolveRequest(kind, n, nrhs, matrix_id, _buf_ptr(A), _buf_ptr(B), _buf_ptr(X))
+        t = _c.c_longlong()
+        _check(_lib.posit_server_submit(self._h, _c.byref(q), _c.byref(t)), "server submit")
+        self._keep[t.value] = (A, B, X)
+        return t.value
+
+    @staticmethod
+    def _result(r):
+        return {"status": r.status, "info": r.info, "cache_hit": bool(r.cache_hit), "path": r.path,
+                "queue_ms": r.queue_ms, "latency_ms": r.latency_ms}
+
+    def wait(self, ticket):
+        r = _SolveResult()
+        _check(_lib.posit_server_wait(self._h, ticket, _c.byref(r)), "server wait")
+        self._keep.pop(ticket, None)
+        return self._result(r)
+
+    def poll(self, ticket):
+        """The result if the request is finished, else None."""
+        r = _SolveResult()
+        rc = _lib.posit_server_poll(self._h, ticket, _c.byref(r))
+        if rc < 0:
+            _check(rc, "server poll")
+        if rc == 0:
+            return None
+        self._keep.pop(ticket, None)
+        return self._result(r)
+
+    def cancel(self, ticket):
+        """True if the request was cancelled before admission."""
+        rc = _lib.posit_server_cancel(self._h, ticket)
+        if rc < 0:
+            _check(rc, "server cancel")
+        return rc == 0
+
+    def stats(self):
+        st = _ServerStats()
+        _check(_lib.posit_server_get_stats(self._h, _c.byref(st)), "server stats")
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.posit_server_destroy(h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()

@@ -11,8 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libposit_gpu_b200.so")
-SOURCES = ["gemm.cu", "lapack.cu", "batch.cu", "batch_gemm.cu", "capi.cu", "batch_capi.cu", "noalloc.cu"]
-HEADERS = ["posit32.cuh", "gemm.cuh", "gemm_tile.cuh", "lapack.cuh", "batch.cuh", "batch_gemm.cuh"]
+SOURCES = ["gemm.cu", "lapack.cu", "batch.cu", "batch_gemm.cu", "capi.cu", "batch_capi.cu", "noalloc.cu", "serve.cu"]
+HEADERS = ["posit32.cuh", "gemm.cuh", "gemm_tile.cuh", "lapack.cuh", "batch.cuh", "batch_gemm.cuh", "trsm_chain.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

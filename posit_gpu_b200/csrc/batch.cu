@@ -10,6 +10,7 @@
 // posit_rpotrs_dev) and to the CPU routines.
 #include "batch.cuh"
 #include "posit32.cuh"
+#include "trsm_chain.cuh"
 
 namespace pg {
 
@@ -49,7 +50,7 @@ __device__ int iramax_block(const uint32_t *col, int k, int n, int32_t *s_key, i
 }
 
 // Rgetrf (as unblocked right-looking LU) + Rgetrs('N') for one problem.
-__device__ void lu_solve_one(const BatchProblem &pr, int32_t *s_key, int *s_idx, uint32_t *s_row)
+__device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key, int *s_idx, uint32_t *s_row)
 {
     const int n = pr.n, tid = threadIdx.x;
     uint32_t *A = pr.A;
@@ -57,7 +58,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, int32_t *s_key, int *s_idx,
     int info = 0;
     __shared__ uint32_t s_piv, s_recip;
     __shared__ int s_mode;
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < (factor ? n : 0); ++k) {
         uint32_t *ck = A + (size_t)k * lda;
         const int p = iramax_block(ck, k, n, s_key, s_idx);
         const uint32_t piv = ck[p];
@@ -106,50 +107,57 @@ __device__ void lu_solve_one(const BatchProblem &pr, int32_t *s_key, int *s_idx,
         }
         __syncthreads();
     }
-    if (tid == 0)
+    if (tid == 0 && factor)
         *pr.info = info;
-    // Rgetrs 'N': interchanges, L (unit) forward, U backward -- per right-hand side
-    for (int r = 0; r < pr.nrhs; ++r) {
-        uint32_t *b = pr.B + (size_t)r * pr.ldb;
-        if (tid == 0)
-            for (int i = 0; i < n; ++i) {
-                int ip = pr.ipiv[i] - 1;
-                if (ip != i) {
-                    uint32_t t = b[i];
-                    b[i] = b[ip];
-                    b[ip] = t;
-                }
+    // Rgetrs 'N': interchanges, L (unit) forward, U backward; the right-hand sides in
+    // parallel (each column's per-element order is Rtrsm's, Rtrsm.cpp:121-154)
+    const int nrhs = pr.nrhs;
+    const size_t ldb = (size_t)pr.ldb;
+    for (int r = tid; r < nrhs; r += blockDim.x) { // Rlaswp, in order, on the own column
+        uint32_t *b = pr.B + (size_t)r * ldb;
+        for (int i = 0; i < n; ++i) {
+            const int ip = pr.ipiv[i] - 1;
+            if (ip != i) {
+                const uint32_t t = b[i];
+                b[i] = b[ip];
+                b[ip] = t;
             }
-        __syncthreads();
-        for (int k = 0; k < n; ++k) {
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const int rows = n - k - 1;
+        const uint32_t *lk = A + (size_t)k * lda;
+        for (int e = tid; e < rows * nrhs; e += blockDim.x) {
+            uint32_t *b = pr.B + (size_t)(e / rows) * ldb;
+            const int i = k + 1 + e % rows;
             const uint32_t bk = b[k];
-            if (bk != 0) {
-                const uint32_t nb = pneg(bk);
-                const uint32_t *lk = A + (size_t)k * lda;
-                for (int i = k + 1 + tid; i < n; i += blockDim.x)
-                    b[i] = padd(b[i], pmul(nb, lk[i]));
-            }
-            __syncthreads();
+            if (bk != 0)
+                b[i] = padd(b[i], pmul(pneg(bk), lk[i]));
         }
-        for (int k = n - 1; k >= 0; --k) {
-            uint32_t bk = b[k];
-            __syncthreads();
-            if (bk != 0) {
-                const uint32_t *uk = A + (size_t)k * lda;
-                bk = pdiv(bk, uk[k]);
-                if (tid == 0)
-                    b[k] = bk;
-                const uint32_t nb = pneg(bk);
-                for (int i = tid; i < k; i += blockDim.x)
-                    b[i] = padd(b[i], pmul(nb, uk[i]));
-            }
-            __syncthreads();
+        __syncthreads();
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        const uint32_t *uk = A + (size_t)k * lda;
+        for (int r = tid; r < nrhs; r += blockDim.x) {
+            uint32_t *b = pr.B + (size_t)r * ldb;
+            if (b[k] != 0)
+                b[k] = pdiv(b[k], uk[k]);
         }
+        __syncthreads();
+        for (int e = tid; e < k * nrhs; e += blockDim.x) {
+            uint32_t *b = pr.B + (size_t)(e / k) * ldb;
+            const int i = e % k;
+            const uint32_t bk = b[k];
+            if (bk != 0)
+                b[i] = padd(b[i], pmul(pneg(bk), uk[i]));
+        }
+        __syncthreads();
     }
 }
 
 // Rpotrf('L') (as unblocked right-looking Cholesky) + Rpotrs('L') for one problem.
-__device__ void chol_solve_one(const BatchProblem &pr, uint32_t *s_row)
+__device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_row)
 {
     const int n = pr.n, tid = threadIdx.x;
     uint32_t *A = pr.A;
@@ -157,7 +165,7 @@ __device__ void chol_solve_one(const BatchProblem &pr, uint32_t *s_row)
     __shared__ uint32_t s_recip;
     __shared__ int s_fail;
     int info = 0;
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < (factor ? n : 0); ++k) {
         uint32_t *ck = A + (size_t)k * lda;
         if (tid == 0) {
             uint32_t akk = ck[k];
@@ -191,42 +199,34 @@ __device__ void chol_solve_one(const BatchProblem &pr, uint32_t *s_row)
         }
         __syncthreads();
     }
-    if (tid == 0)
+    if (tid == 0 && factor)
         *pr.info = info;
     if (info != 0)
         return;
-    for (int r = 0; r < pr.nrhs; ++r) {
-        uint32_t *b = pr.B + (size_t)r * pr.ldb;
-        // L forward, non-unit: b_k /= l_kk, then b_i -= b_k*l_ik
-        for (int k = 0; k < n; ++k) {
-            uint32_t bk = b[k];
-            __syncthreads();
-            if (bk != 0) {
-                const uint32_t *lk = A + (size_t)k * lda;
-                bk = pdiv(bk, lk[k]);
-                if (tid == 0)
-                    b[k] = bk;
-                const uint32_t nb = pneg(bk);
-                for (int i = k + 1 + tid; i < n; i += blockDim.x)
-                    b[i] = padd(b[i], pmul(nb, lk[i]));
-            }
-            __syncthreads();
+    // Rpotrs 'L': L forward (Rtrsm.cpp:139-154, non-unit), the right-hand sides in
+    // parallel; then L^T backward, one thread's chain per right-hand side (trsm_chain.cuh)
+    const int nrhs = pr.nrhs;
+    const size_t ldb = (size_t)pr.ldb;
+    for (int k = 0; k < n; ++k) {
+        const uint32_t *lk = A + (size_t)k * lda;
+        for (int r = tid; r < nrhs; r += blockDim.x) {
+            uint32_t *b = pr.B + (size_t)r * ldb;
+            if (b[k] != 0)
+                b[k] = pdiv(b[k], lk[k]);
         }
-        // L^T backward: t = b_i - sum_{k>i} l_ki*b_k (k ascending), b_i = t / l_ii
-        for (int i = n - 1; i >= 0; --i) {
-            const uint32_t *li = A + (size_t)i * lda;
-            for (int k = i + 1 + tid; k < n; k += blockDim.x)
-                s_row[k] = pmul(li[k], b[k]);
-            __syncthreads();
-            if (tid == 0) {
-                uint32_t t = b[i];
-                for (int k = i + 1; k < n; ++k)
-                    t = psub(t, s_row[k]);
-                b[i] = pdiv(t, li[i]);
-            }
-            __syncthreads();
+        __syncthreads();
+        const int rows = n - k - 1;
+        for (int e = tid; e < rows * nrhs; e += blockDim.x) {
+            uint32_t *b = pr.B + (size_t)(e / rows) * ldb;
+            const int i = k + 1 + e % rows;
+            const uint32_t bk = b[k];
+            if (bk != 0)
+                b[i] = padd(b[i], pmul(pneg(bk), lk[i]));
         }
+        __syncthreads();
     }
+    for (int r = tid; r < nrhs; r += blockDim.x)
+        llt_chain(A, lda, pr.B + (size_t)r * ldb, n, false);
 }
 
 } // namespace
@@ -247,10 +247,11 @@ __global__ void __launch_bounds__(BT) batch_factor_kernel(const BatchProblem *__
         if (item >= nprob)
             return;
         const BatchProblem pr = probs[order ? order[item] : item];
-        if (pr.kind == BATCH_LU)
-            lu_solve_one(pr, s_key, s_idx, s_row);
+        const bool factor = !(pr.kind & BATCH_SOLVE_ONLY);
+        if ((pr.kind & 1) == BATCH_LU)
+            lu_solve_one(pr, factor, s_key, s_idx, s_row);
         else
-            chol_solve_one(pr, s_row);
+            chol_solve_one(pr, factor, s_row);
         __syncthreads();
     }
 }

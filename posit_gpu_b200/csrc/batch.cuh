@@ -12,8 +12,10 @@ constexpr int BATCH_MAX_N = 4096; // largest n a batched problem may have
 // One problem: A (n x n, column-major, lda) is factored in place, B (n x nrhs, ldb)
 // overwritten with the solution; ipiv (LU) receives n 1-based pivots, info the
 // reference's info.  All pointers are device pointers.
+constexpr int BATCH_SOLVE_ONLY = 2; // flag added to kind: A (and ipiv) already factored
+
 struct BatchProblem {
-    int kind;
+    int kind; // BATCH_LU or BATCH_CHOL, plus BATCH_SOLVE_ONLY
     int n, lda, nrhs, ldb;
     uint32_t *A;
     uint32_t *B;

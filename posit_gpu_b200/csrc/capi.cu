@@ -513,6 +513,16 @@ const char *posit_strerror(int code)
         return "variant not implemented on the device";
     case POSIT_E_NOALLOC_LIMIT:
         return "shape needs more scratch than the allocation-free entry point's static array";
+    case POSIT_E_QUEUE_FULL:
+        return "server queue full";
+    case POSIT_E_CANCELLED:
+        return "request cancelled";
+    case POSIT_E_NOT_CACHED:
+        return "no factor cached under this matrix id";
+    case POSIT_E_MISMATCH:
+        return "matrix id cached with another kind or order";
+    case POSIT_E_UNKNOWN_TICKET:
+        return "unknown ticket";
     default:
         if (code > 0)
             return "illegal argument (BLAS info = parameter number)";

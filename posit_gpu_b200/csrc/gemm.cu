@@ -25,6 +25,7 @@
 #include "gemm_tile.cuh"
 #include "posit32.cuh"
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -310,7 +311,7 @@ __global__ void scale_kernel(int m, int n, uint32_t beta, uint32_t *__restrict__
 // ---------------------------------------------------------------------------
 namespace {
 std::mutex g_prof_mu;
-bool g_prof_on = false;
+std::atomic<bool> g_prof_on{false};
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
 double g_prof_ms = 0.0;
 long long g_prof_main = 0, g_prof_all = 0;
@@ -464,6 +465,8 @@ cudaError_t convert_launch(bool to_posit, const void *in, void *out, size_t n, c
     prof_count(1);
     return cudaGetLastError();
 }
+
+cudaError_t device_error_address(int **p) { return cudaGetSymbolAddress((void **)p, g_dev_error); }
 
 int read_device_error(bool clear)
 {

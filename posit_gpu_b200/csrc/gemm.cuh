@@ -49,6 +49,8 @@ cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cuda
 cudaError_t convert_launch(bool to_posit, const void *in, void *out, size_t n, cudaStream_t stream);
 
 int read_device_error(bool clear);
+// Device address of the kernels' error flag (for stream-ordered copies of it).
+cudaError_t device_error_address(int **p);
 
 // Optional instrumentation: CUDA events around each main-kernel launch, recorded on
 // the launch stream, plus a count of this library's kernel launches.

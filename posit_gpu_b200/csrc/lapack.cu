@@ -23,6 +23,7 @@
 #include "gemm.cuh"
 #include "lapack.cuh"
 #include "posit32.cuh"
+#include "trsm_chain.cuh"
 
 namespace pg {
 
@@ -234,38 +235,17 @@ __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint
         bcol[i] = s_b[i];
 }
 
-// Lower, transposed, non-unit (Rtrsm.cpp:175-186): for i = m-1..0,
-// t = b_i - sum_{k>i} a_ki*b_k (k ascending), b_i = t / a_ii.  Each b_i's sum starts with
-// the b_{i+1} just computed, so the whole solve is one dependent chain; the products
-// are computed by the CTA ahead of the chain and one thread runs the chain of additions.
-__global__ void trsm_llt_kernel(const uint32_t *__restrict__ L, size_t ldl, uint32_t *__restrict__ B, size_t ldb,
-                                int m, bool unit, const int *__restrict__ info)
+// Lower, transposed (Rtrsm.cpp:175-186): one thread per right-hand side runs the whole
+// dependent chain (trsm_chain.cuh); 32 right-hand sides per block.
+__global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict__ L, size_t ldl,
+                                                      uint32_t *__restrict__ B, size_t ldb, int m, int nrhs,
+                                                      bool unit, const int *__restrict__ info)
 {
-    extern __shared__ uint32_t s_b[]; // [0, m): b; [m, 2m): products of the current row
     if (info && *info < 0)
         return;
-    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
-    uint32_t *s_p = s_b + m;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        s_b[i] = bcol[i];
-    __syncthreads();
-    for (int i = m - 1; i >= 0; --i) {
-        const uint32_t *li = L + (size_t)i * ldl; // column i of L: a_ki for k > i
-        for (int k = i + 1 + threadIdx.x; k < m; k += blockDim.x)
-            s_p[k] = pmul(li[k], s_b[k]);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t t = s_b[i]; // alpha*b with alpha == 1
-            for (int k = i + 1; k < m; ++k)
-                t = psub(t, s_p[k]);
-            if (!unit)
-                t = pdiv(t, li[i]);
-            s_b[i] = t;
-        }
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        bcol[i] = s_b[i];
+    const int r = blockIdx.x * 32 + threadIdx.x;
+    if (r < nrhs)
+        llt_chain(L, ldl, B + (size_t)r * ldb, m, unit);
 }
 
 // ---------------------------------------------------------------------------
@@ -437,8 +417,6 @@ static cudaError_t solve_smem(size_t bytes)
     cudaError_t e = cudaFuncSetAttribute(trsm_lln_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(trsm_lun_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(trsm_llt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return e;
 }
 
@@ -459,11 +437,11 @@ cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int
 cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
 {
     const int threads = 1024;
-    cudaError_t e = solve_smem((size_t)n * 8);
+    cudaError_t e = solve_smem((size_t)n * 4);
     if (e != cudaSuccess)
         return e;
     trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
-    trsm_llt_kernel<<<nrhs, threads, (size_t)n * 8, st>>>(A, lda, B, ldb, n, false, nullptr);
+    trsm_llt_kernel<<<(nrhs + 31) / 32, 32, 0, st>>>(A, lda, B, ldb, n, nrhs, false, nullptr);
     return cudaGetLastError();
 }
 

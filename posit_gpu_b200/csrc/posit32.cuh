@@ -20,9 +20,11 @@
 
 #if defined(__CUDACC__)
 #define PG_HD __host__ __device__ __forceinline__
+#define PG_HD_MEMBER __host__ __device__ __forceinline__
 #define PG_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define PG_HD static inline
+#define PG_HD_MEMBER inline
 #define PG_HD_NOINLINE static
 #endif
 
@@ -423,16 +425,28 @@ PG_HD RegimeEntry regime_entry(int32_t s)
     return e;
 }
 
+// Regime entry from the shared-memory table (throughput: the GEMM inner loops) or by
+// arithmetic (latency: one thread's chain of dependent additions, where a table load
+// would sit on the dependent path).
+struct TableEntry {
+    const RegimeEntry *tbl;
+    PG_HD_MEMBER RegimeEntry operator()(int32_t s) const { return tbl[s]; }
+};
+struct ComputedEntry {
+    PG_HD_MEMBER RegimeEntry operator()(int32_t s) const { return regime_entry(s); }
+};
+
 // t*a rounded to posit32 (kernel_entry.cl:399-538), both operands decoded and nonzero
 // or decoded zeros.  `bad` gets bit 30 set when the result must come from the exact path
 // (regime longer than 27 bits, or rounding carried out of the significand).
-PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
+template <class EntryOf>
+PG_HD void dmul_core(const dp32 &t, const dp32 &a, EntryOf entry_of, dp32 &r, uint32_t &bad)
 {
     uint64_t P = (uint64_t)t.g * a.g; // hidden bit at 60, or 61 ("carry")
     uint32_t hi = (uint32_t)(P >> 32), lo = (uint32_t)P;
     uint32_t carry = umulhi(hi, 8u);
     int32_t s = t.s + a.s + (int32_t)carry;
-    const RegimeEntry e = tbl[s];
+    const RegimeEntry e = entry_of(s);
     uint32_t W = e.r0 + carry * e.nr1; // 2^(32 - run - carry)
     // T = P >> (run + carry): kept bits in thi (hidden at 28-run), guard+sticky in tlo
     uint32_t thi = umulhi(hi, W);
@@ -441,6 +455,11 @@ PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 
     r.s = s;
     r.x = t.x ^ a.x;
     bad = e.w | (~r.g & e.nr1);
+}
+
+PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
+{
+    dmul_core(t, a, TableEntry{tbl}, r, bad);
 }
 
 // c + p rounded to posit32 (kernel_entry.cl:370-397), both decoded.  Fails (bit 30 of
@@ -453,7 +472,8 @@ PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 
 // a difference A - e (0 < e < 2^32) borrows ones through every bit up to A's last kept
 // bit, so guard and sticky are set and it rounds up to A again -- including when A is a
 // power of two, since the spacing below A is at least 2^(33+run) frame units.
-PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
+template <class EntryOf>
+PG_HD void dadd_core(const dp32 &c, const dp32 &p, EntryOf entry_of, dp32 &r, uint32_t &bad)
 {
     // order by magnitude: scale, then significand (so the difference is never negative).
     // Bitwise, not short-circuit, operators: the latter compile to branches, which both
@@ -472,7 +492,7 @@ PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 
     uint32_t shi = (uint32_t)(S >> 32), slo = (uint32_t)S;
     uint32_t lz = clz32(shi);         // S.hi == 0 only when S == 0
     int32_t s = bs + 3 - (int32_t)lz; // result scale
-    const RegimeEntry e = tbl[s];
+    const RegimeEntry e = entry_of(s);
     uint32_t p2 = shl32(1u, lz);
     uint32_t nhi = shi * p2 + umulhi(slo, p2); // N = S << lz: hidden bit at 63
     uint32_t nlo = slo * p2;
@@ -482,6 +502,11 @@ PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 
     r.s = s;
     r.x = bx;
     bad = e.w | (~r.g & e.nr1);
+}
+
+PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
+{
+    dadd_core(c, p, TableEntry{tbl}, r, bad);
 }
 
 // Exact decoded operations (through patterns): the slow path.  Decoded zeros of the
@@ -510,6 +535,23 @@ PG_HD dp32 dmac(const dp32 &c, const dp32 &t, const dp32 &a, const RegimeEntry *
     uint32_t bm, ba;
     dmul_fast(t, a, tbl, p, bm);
     dadd_fast(c, p, tbl, r, ba);
+    if ((bm | ba) & 0x40000000u)
+        r = dmac_exact(c, t, a);
+    return r;
+}
+
+// c + t*a with both roundings, for one thread's chain of dependent multiply-adds (the
+// dot-form triangular solve, Rtrsm.cpp:175-186, as c - l*b = c + (-b)*l).  Only the
+// addition depends on the previous step; the product, the operands' decoding and the
+// exactness test are independent of it and overlap the chain.  Regime entries are
+// computed (no table load on the dependent path); flagged steps go through the exact
+// routines.  Never fails.
+PG_HD dp32 dmac_chain(const dp32 &c, const dp32 &t, const dp32 &a)
+{
+    dp32 p, r;
+    uint32_t bm, ba;
+    dmul_core(t, a, ComputedEntry{}, p, bm);
+    dadd_core(c, p, ComputedEntry{}, r, ba);
     if ((bm | ba) & 0x40000000u)
         r = dmac_exact(c, t, a);
     return r;

@@ -52,4 +52,32 @@ void hc_chain(const uint32_t *c0, const uint32_t *t, const uint32_t *a, uint32_t
         o[j] = encode(c);
     }
 }
+// c + t*a through the triangular-solve chain step (computed regime entries; NaR outside)
+void hc_dmac_chain_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, uint32_t *o, long n)
+{
+    for (long i = 0; i < n; i++) {
+        if (c[i] == P32_NAR || t[i] == P32_NAR || a[i] == P32_NAR) {
+            o[i] = P32_NAR;
+            continue;
+        }
+        o[i] = encode(dmac_chain(decode_gemm(c[i]), decode_gemm(t[i]), decode_gemm(a[i])));
+    }
+}
+// one right-hand side of the L^T solve (trsm_chain.cuh's loop, on the host)
+void hc_llt_solve(const uint32_t *L, long ld, uint32_t *b, int m)
+{
+    for (int i = m - 1; i >= 0; --i) {
+        const uint32_t *li = L + (long)i * ld;
+        const uint32_t bi = b[i];
+        uint32_t nar = bi == P32_NAR;
+        dp32 c = decode_gemm(nar ? 0u : bi);
+        for (int k = i + 1; k < m; ++k) {
+            const uint32_t l = li[k], bk = b[k];
+            nar |= (l == P32_NAR) | (bk == P32_NAR);
+            c = dmac_chain(c, decode_gemm(bk == P32_NAR ? 0u : 0u - bk), decode_gemm(l == P32_NAR ? 0u : l));
+        }
+        uint32_t t = nar ? P32_NAR : encode(c);
+        b[i] = pdiv(t, li[i]);
+    }
+}
 }

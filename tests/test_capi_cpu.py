@@ -85,3 +85,19 @@ def test_strerror_and_workspace_size():
     assert ws >= 8 * (100 + 70) * 33 + 100 + 70
     assert ws < 8 * (100 + 70 + 2 * 64) * (33 + 16) + 1024
     assert pg.workspace_size("N", "T", 100, 70, 66) > ws
+
+
+def test_server_needs_a_device_and_reports_it():
+    """Without a GPU the request loop is not started: creation returns POSIT_E_NO_DEVICE
+    and no thread or allocation is left behind."""
+    import torch
+
+    import posit_gpu_b200 as pg
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pg.PositError, match="no usable CUDA device"):
+        pg.Server()
+    for code, text in ((pg.E_QUEUE_FULL, b"queue"), (pg.E_CANCELLED, b"cancelled"),
+                       (pg.E_NOT_CACHED, b"cached"), (pg.E_MISMATCH, b"matrix id"),
+                       (pg.E_UNKNOWN_TICKET, b"ticket")):
+        assert text in pg._lib.posit_strerror(code)

@@ -28,6 +28,8 @@ def hc(tmp_path_factory):
     lib.hc_dmac_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
     lib.hc_dmac_n.restype = ctypes.c_long
     lib.hc_chain.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_long]
+    lib.hc_dmac_chain_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
+    lib.hc_llt_solve.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
     return lib
 
 
@@ -100,3 +102,41 @@ def test_decoded_chains_match_oracle(hc):
         oracle.orc.orc_p32_mul_n(np.ascontiguousarray(t[l::ln]), np.ascontiguousarray(a[l::ln]), p, nch)
         oracle.orc.orc_p32_add_n(want, p, want, nch)
     assert np.array_equal(out, want)
+
+
+def test_chain_multiply_add_step_matches_oracle(hc):
+    """The triangular-solve chain step c + t*a (computed regime entries, exact fallback)
+    equals p32_add(c, p32_mul(t, a)) on random, wide-range, long-regime, cancelling and
+    special operands."""
+    rng = np.random.default_rng(5)
+    c, t, a = _mix(rng, 40_000), _mix(rng, 40_000), _mix(rng, 40_000)
+    a[::7] = oracle.P32_ONE
+    c[::7] = (0 - t[::7].astype(np.uint64)).astype(np.uint32)  # c - t*1 == 0: exact cancellation
+    out = np.empty_like(c)
+    hc.hc_dmac_chain_n(c, t, a, out, c.size)
+    p = np.empty_like(c)
+    oracle.orc.orc_p32_mul_n(t, a, p, c.size)
+    want = np.empty_like(c)
+    oracle.orc.orc_p32_add_n(c, p, want, c.size)
+    assert np.array_equal(out, want)
+
+
+def test_lower_transposed_solve_matches_oracle(hc):
+    """trsm_chain.cuh's L^T solve, run on the host, against the oracle's Rtrsm('L', 'L',
+    'T', 'N') on Cholesky-like and wide-range triangles, with zeros and a NaR."""
+    rng = np.random.default_rng(6)
+    for m, kind in ((1, "u"), (9, "u"), (120, "u"), (64, "w"), (50, "nar")):
+        L = oracle.from_double(rng.uniform(-1, 1, m * m))
+        if kind == "w":
+            L = oracle.from_double(np.sign(rng.uniform(-1, 1, m * m)) * 10.0 ** rng.uniform(-20, 20, m * m))
+        for i in range(m):
+            L[i + i * m] = oracle.p32(1.0 + rng.uniform(0, 1))
+        b = oracle.from_double(rng.uniform(-1, 1, m))
+        b[::5] = 0
+        if kind == "nar":
+            L[(m - 1) + 3 * m] = oracle.P32_NAR
+        got = b.copy()
+        hc.hc_llt_solve(L, m, got, m)
+        want = b.copy()
+        oracle.orc.orc_rtrsm(b"L", b"L", b"T", b"N", m, 1, oracle.P32_ONE, L, m, want, m)
+        assert np.array_equal(got, want), (m, kind)
