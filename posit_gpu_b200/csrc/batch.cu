@@ -225,8 +225,18 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
         }
         __syncthreads();
     }
+    // L^T backward: the right-hand sides staged in shared memory when they fit
+    const bool staged = n * nrhs <= BATCH_MAX_N;
+    if (staged)
+        for (int e = tid; e < n * nrhs; e += blockDim.x)
+            s_row[e] = pr.B[(size_t)(e / n) * ldb + e % n];
+    __syncthreads();
     for (int r = tid; r < nrhs; r += blockDim.x)
-        llt_chain(A, lda, pr.B + (size_t)r * ldb, n, false);
+        llt_chain(A, lda, staged ? s_row + (size_t)r * n : pr.B + (size_t)r * ldb, n, false);
+    __syncthreads();
+    if (staged)
+        for (int e = tid; e < n * nrhs; e += blockDim.x)
+            pr.B[(size_t)(e / n) * ldb + e % n] = s_row[e];
 }
 
 } // namespace

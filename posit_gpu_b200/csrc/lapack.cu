@@ -235,18 +235,92 @@ __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint
         bcol[i] = s_b[i];
 }
 
-// Lower, transposed (Rtrsm.cpp:175-186): one thread per right-hand side runs the whole
-// dependent chain (trsm_chain.cuh); 32 right-hand sides per block.
+// Lower, transposed (Rtrsm.cpp:175-186): one block per right-hand side; the column is
+// staged in shared memory (when it fits) and one thread runs the whole dependent chain
+// (trsm_chain.cuh).
+constexpr int LLT_SMEM_MAX = 227 * 1024;
+
 __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict__ L, size_t ldl,
-                                                      uint32_t *__restrict__ B, size_t ldb, int m, int nrhs,
+                                                      uint32_t *__restrict__ B, size_t ldb, int m, bool staged,
                                                       bool unit, const int *__restrict__ info)
 {
+    extern __shared__ uint32_t s_col[];
     if (info && *info < 0)
         return;
-    const int r = blockIdx.x * 32 + threadIdx.x;
-    if (r < nrhs)
-        llt_chain(L, ldl, B + (size_t)r * ldb, m, unit);
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    if (!staged) {
+        if (threadIdx.x == 0)
+            llt_chain(L, ldl, bcol, m, unit);
+        return;
+    }
+    for (int i = threadIdx.x; i < m; i += 32)
+        s_col[i] = bcol[i];
+    __syncwarp();
+    if (threadIdx.x == 0)
+        llt_chain(L, ldl, s_col, m, unit);
+    __syncwarp();
+    for (int i = threadIdx.x; i < m; i += 32)
+        bcol[i] = s_col[i];
 }
+
+// The same solve split over warps (one block per right-hand side, column length m with
+// 20*m bytes of shared memory): lane 0 of warp 0 runs the chain of additions for row i
+// while warps 1..3 compute the decoded terms -a_k,i-1 * b_k of row i-1 (all but its first
+// term, whose b_i the chain is still producing) into the other half of a double buffer.
+// One barrier per row.  The chain thread forms the first term of each row itself.
+constexpr int LLT_PC_THREADS = 128;
+
+__global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint32_t *__restrict__ L, size_t ldl,
+                                                                     uint32_t *__restrict__ B, size_t ldb, int m,
+                                                                     bool unit, const int *__restrict__ info)
+{
+    extern __shared__ __align__(16) unsigned char smem_pc[];
+    PackedDp *s_q = reinterpret_cast<PackedDp *>(smem_pc); // [2][m]
+    uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
+    __shared__ uint32_t s_nar[2];
+    if (info && *info < 0)
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    const int tid = threadIdx.x;
+    for (int k = tid; k < m; k += LLT_PC_THREADS)
+        s_b[k] = bcol[k];
+    if (tid < 2)
+        s_nar[tid] = 0;
+    __syncthreads();
+    for (int i = m - 1; i >= 0; --i) {
+        const int cur = i & 1;
+        if (tid == 0) {
+            const uint32_t *li = L + (size_t)i * ldl;
+            const uint32_t bi = s_b[i];
+            uint32_t nar = (bi == P32_NAR) | s_nar[cur];
+            dp32 c = decode_gemm(bi == P32_NAR ? 0u : bi);
+            if (i + 1 < m) {
+                const PackedDp q0 = llt_term(li[i + 1], s_b[i + 1], &nar);
+                c = chain_add_run(c, &q0, 1);
+                c = chain_add_run(c, s_q + (size_t)cur * m + (i + 2), m - i - 2);
+            }
+            uint32_t t = nar ? P32_NAR : encode(c);
+            if (!unit)
+                t = pdiv(t, li[i]);
+            s_b[i] = t;
+            s_nar[cur] = 0;
+        } else if (tid >= 32 && i >= 1) {
+            // terms k = i+1 .. m-1 of row i-1 (their b_k are final)
+            const uint32_t *lp = L + (size_t)(i - 1) * ldl;
+            PackedDp *qn = s_q + (size_t)(cur ^ 1) * m;
+            uint32_t nar = 0;
+            for (int k = i + 1 + (tid - 32); k < m; k += LLT_PC_THREADS - 32)
+                qn[k] = llt_term(lp[k], s_b[k], &nar);
+            if (nar)
+                s_nar[cur ^ 1] = 1;
+        }
+        __syncthreads();
+    }
+    for (int k = tid; k < m; k += LLT_PC_THREADS)
+        bcol[k] = s_b[k];
+}
+
+size_t llt_pc_smem_bytes(int m) { return (size_t)m * (2 * sizeof(PackedDp) + 4); }
 
 // ---------------------------------------------------------------------------
 // Cholesky panel (lower)
@@ -441,7 +515,24 @@ cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uin
     if (e != cudaSuccess)
         return e;
     trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
-    trsm_llt_kernel<<<(nrhs + 31) / 32, 32, 0, st>>>(A, lda, B, ldb, n, nrhs, false, nullptr);
+    const size_t pc = llt_pc_smem_bytes(n);
+    if (pc <= (size_t)LLT_SMEM_MAX) {
+        if (pc > 48 * 1024) {
+            e = cudaFuncSetAttribute(trsm_llt_pc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc);
+            if (e != cudaSuccess)
+                return e;
+        }
+        trsm_llt_pc_kernel<<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
+        return cudaGetLastError();
+    }
+    const size_t col = (size_t)n * 4;
+    const bool staged = col <= (size_t)LLT_SMEM_MAX;
+    if (staged && col > 48 * 1024) {
+        e = cudaFuncSetAttribute(trsm_llt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col);
+        if (e != cudaSuccess)
+            return e;
+    }
+    trsm_llt_kernel<<<nrhs, 32, staged ? col : 0, st>>>(A, lda, B, ldb, n, staged, false, nullptr);
     return cudaGetLastError();
 }
 

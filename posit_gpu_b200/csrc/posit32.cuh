@@ -415,13 +415,15 @@ constexpr int32_t RT_N = RT_MAX - RT_MIN + 1;
 PG_HD RegimeEntry regime_entry(int32_t s)
 {
     RegimeEntry e;
-    bool zero_region = s < ZERO_REGION;
-    bool fast = in_fast_range(s);
-    uint32_t run = (fast && !zero_region) ? regime_run(s) : 27u;
+    // bitwise, not short-circuit, operators: this also runs on a dependent path, where a
+    // branch would stop independent work from overlapping it
+    const bool zero_region = s < ZERO_REGION;
+    const bool fast = in_fast_range(s); // the fast window lies above the zero region
+    const uint32_t run = fast ? regime_run(s) : 27u;
     e.r0 = 1u << (32 - run);
     e.nr1 = zero_region ? 0u : 0u - (1u << (31 - run));
     e.g = 1u << (run + 2);
-    e.w = (1u << (29 - run)) | ((fast || zero_region) ? 0u : 0x40000000u);
+    e.w = (1u << (29 - run)) | ((fast | zero_region) ? 0u : 0x40000000u);
     return e;
 }
 
@@ -526,6 +528,25 @@ PG_HD dp32 decode_gemm(uint32_t u)
     if (u == 0)
         d.s = GEMM_ZERO_SCALE;
     return d;
+}
+
+// decode_gemm without branches (selects only), for a thread's dependent chain, where a
+// branch would stop the next step's independent work from overlapping the current one.
+// u must not be NaR.
+PG_HD dp32 decode_gemm_bf(uint32_t u)
+{
+    const uint32_t x = u >> 31;
+    const uint32_t v = x ? 0u - u : u;
+    const uint32_t y = v << 1;
+    const uint32_t ones = v & 0x40000000u;
+    const uint32_t run = clz32(ones ? ~y : y);
+    const int32_t k = ones ? (int32_t)run - 1 : -(int32_t)run;
+    const uint32_t rest = shl32(v, run + 2); // exponent at 31..30, fraction below
+    dp32 r;
+    r.s = u == 0 ? GEMM_ZERO_SCALE : 4 * k + (int32_t)(rest >> 30);
+    r.g = u == 0 ? 0u : (P32_ONE | (rest & 0x3FFFFFFFu));
+    r.x = x;
+    return r;
 }
 
 // c + t*a with both roundings; never fails.  tbl points at the entry for scale 0.

@@ -1,6 +1,7 @@
 // Host build of the product's posit32 arithmetic (posit_gpu_b200/csrc/posit32.cuh) for
 // CPU tests against the oracle.  Compiled by tests/test_posit_core_cpu.py.
 #include "../posit_gpu_b200/csrc/posit32.cuh"
+#include "../posit_gpu_b200/csrc/trsm_chain.cuh"
 #include <stdint.h>
 using namespace pg;
 static RegimeEntry g_table[RT_N];
@@ -63,21 +64,47 @@ void hc_dmac_chain_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, ui
         o[i] = encode(dmac_chain(decode_gemm(c[i]), decode_gemm(t[i]), decode_gemm(a[i])));
     }
 }
-// one right-hand side of the L^T solve (trsm_chain.cuh's loop, on the host)
-void hc_llt_solve(const uint32_t *L, long ld, uint32_t *b, int m)
+// one right-hand side of the L^T solve: trsm_chain.cuh's llt_chain, built for the host
+void hc_llt_solve(const uint32_t *L, long ld, uint32_t *b, int m) { llt_chain(L, (size_t)ld, b, m, false); }
+// decode_gemm_bf against decode_gemm on n patterns (NaR skipped); returns mismatches
+long hc_decode_bf_mismatch(const uint32_t *u, long n)
 {
+    long bad = 0;
+    for (long i = 0; i < n; i++) {
+        if (u[i] == P32_NAR)
+            continue;
+        const dp32 a = decode_gemm(u[i]), b = decode_gemm_bf(u[i]);
+        bad += (a.s != b.s) | (a.g != b.g) | (a.x != b.x);
+    }
+    return bad;
+}
+// the split L^T solve (products as llt_term, additions as chain_add_run), row by row
+void hc_llt_solve_split(const uint32_t *L, long ld, uint32_t *b, int m)
+{
+    PackedDp *q = new PackedDp[m > 0 ? m : 1];
     for (int i = m - 1; i >= 0; --i) {
         const uint32_t *li = L + (long)i * ld;
-        const uint32_t bi = b[i];
-        uint32_t nar = bi == P32_NAR;
-        dp32 c = decode_gemm(nar ? 0u : bi);
-        for (int k = i + 1; k < m; ++k) {
-            const uint32_t l = li[k], bk = b[k];
-            nar |= (l == P32_NAR) | (bk == P32_NAR);
-            c = dmac_chain(c, decode_gemm(bk == P32_NAR ? 0u : 0u - bk), decode_gemm(l == P32_NAR ? 0u : l));
+        uint32_t nar = b[i] == P32_NAR;
+        for (int k = i + 1; k < m; ++k)
+            q[k] = llt_term(li[k], b[k], &nar);
+        dp32 c = decode_gemm(b[i] == P32_NAR ? 0u : b[i]);
+        if (i + 1 < m) {
+            c = chain_add_run(c, q + i + 1, 1);
+            c = chain_add_run(c, q + i + 2, m - i - 2);
         }
         uint32_t t = nar ? P32_NAR : encode(c);
         b[i] = pdiv(t, li[i]);
     }
+    delete[] q;
+}
+// chain_add_run over n terms from patterns (NaR excluded by the caller)
+uint32_t hc_chain_add(uint32_t c0, const uint32_t *q, int n)
+{
+    PackedDp *d = new PackedDp[n > 0 ? n : 1];
+    for (int k = 0; k < n; ++k)
+        d[k] = pack_q(decode_gemm(q[k]));
+    uint32_t r = encode(chain_add_run(decode_gemm(c0), d, n));
+    delete[] d;
+    return r;
 }
 }

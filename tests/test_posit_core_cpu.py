@@ -30,6 +30,11 @@ def hc(tmp_path_factory):
     lib.hc_chain.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_long]
     lib.hc_dmac_chain_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
     lib.hc_llt_solve.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
+    lib.hc_llt_solve_split.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
+    lib.hc_chain_add.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
+    lib.hc_chain_add.restype = ctypes.c_uint32
+    lib.hc_decode_bf_mismatch.argtypes = [U32, ctypes.c_long]
+    lib.hc_decode_bf_mismatch.restype = ctypes.c_long
     return lib
 
 
@@ -135,8 +140,41 @@ def test_lower_transposed_solve_matches_oracle(hc):
         b[::5] = 0
         if kind == "nar":
             L[(m - 1) + 3 * m] = oracle.P32_NAR
-        got = b.copy()
-        hc.hc_llt_solve(L, m, got, m)
         want = b.copy()
         oracle.orc.orc_rtrsm(b"L", b"L", b"T", b"N", m, 1, oracle.P32_ONE, L, m, want, m)
-        assert np.array_equal(got, want), (m, kind)
+        for solve in (hc.hc_llt_solve, hc.hc_llt_solve_split):
+            got = b.copy()
+            solve(L, m, got, m)
+            assert np.array_equal(got, want), (m, kind, solve.__name__)
+
+
+def test_branch_free_decode_matches_decode(hc):
+    """The chain's select-only decode equals the GEMM decode on every pattern class:
+    random, all regime lengths (each power of two and its neighbours), zero, extremes."""
+    rng = np.random.default_rng(8)
+    pw = np.array([1 << i for i in range(31)], dtype=np.uint64)
+    edges = np.concatenate([pw, pw - 1, pw + 1, 0x80000000 - pw, 0x80000000 + pw, 0xFFFFFFFF - pw + 1]) % (1 << 32)
+    u = np.concatenate([_mix(rng, 100_000), edges.astype(np.uint32),
+                        np.array([0, 1, 0x7FFFFFFF, 0x80000001, 0xFFFFFFFF, 0x40000000, 0xC0000000], np.uint32)])
+    assert hc.hc_decode_bf_mismatch(np.ascontiguousarray(u), u.size) == 0
+
+
+def test_chain_of_additions_matches_oracle(hc):
+    """chain_add_run (blocks without a branch, failed blocks replayed exactly) equals the
+    reference's p32_add applied in order, on runs that cancel, go wide and hit zero."""
+    rng = np.random.default_rng(12)
+    for trial in range(300):
+        n = int(rng.integers(0, 70))
+        kind = trial % 3
+        if kind == 0:
+            q = oracle.from_double(rng.uniform(-1, 1, n))
+        elif kind == 1:
+            q = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 10.0 ** rng.uniform(-40, 40, n))
+        else:  # values that cancel the running sum exactly now and then
+            q = oracle.from_double(rng.choice([-1.0, 1.0, 0.5, -0.5, 0.0, 3.0, -3.0], n))
+        c0 = int(oracle.from_double(np.array([rng.uniform(-2, 2)]))[0])
+        want = np.array([c0], np.uint32)
+        for k in range(n):
+            oracle.orc.orc_p32_add_n(want, q[k:k + 1].copy(), want, 1)
+        assert hc.hc_chain_add(c0, np.ascontiguousarray(q), n) == int(want[0]), (trial, n)
+
