@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--rates", default="5,10,20,40,burst", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--per-call-sample", type=int, default=100, help="serve: requests timed on the per-call path")
     ap.add_argument("--batch-max-n", type=int, default=0, help="serve: batched-kernel size limit (0: default)")
+    ap.add_argument("--lanes", type=int, default=0, help="serve: CUDA streams of the server (0: default)")
+    ap.add_argument("--launch-threads", type=int, default=0, help="serve: launcher threads (0: default)")
     return ap.parse_args()
 
 
@@ -672,7 +674,7 @@ def serve_arm(args):
         arng = np.random.default_rng(77)
         gaps = np.zeros(R) if rate == "burst" else arng.exponential(1.0 / float(rate), R)
         arrive = np.cumsum(gaps) - gaps[0]
-        with pg.Server(batch_max_n=args.batch_max_n) as srv:
+        with pg.Server(batch_max_n=args.batch_max_n, lanes=args.lanes, launch_threads=args.launch_threads) as srv:
             tickets, t_sub = [None] * R, [0.0] * R
 
             def feed():
@@ -694,8 +696,12 @@ def serve_arm(args):
         ok = all(x["status"] == 0 for x in res)
         hits = sum(x["cache_hit"] for x in res)
         xs_run = [o.numpy().view(np.uint32) for o in outs]
-        same_pc = all(res[i]["info"] == pc_info[i] and (pc_info[i] != 0 or np.array_equal(xs_run[i], xs[i]))
-                      for i in range(S))
+        bad_pc = [i for i in range(S)
+                  if res[i]["info"] != pc_info[i] or (pc_info[i] == 0 and not np.array_equal(xs_run[i], xs[i]))]
+        same_pc = not bad_pc
+        mismatches = [{"i": i, "kind": reqs[i][0], "n": reqs[i][1], "nrhs": reqs[i][2], "path": res[i]["path"],
+                       "hit": res[i]["cache_hit"], "info": res[i]["info"], "want_info": pc_info[i]}
+                      for i in bad_pc[:8]]
         if served_x is None:
             served_x = (xs_run, [x["info"] for x in res])
         else:
@@ -715,7 +721,8 @@ def serve_arm(args):
                      "all_ok": ok, "cache_hits": hits, "inflight_peak": st["inflight_peak"],
                      "batched_units": st["batched_units"], "blocked_units": st["blocked_units"],
                      "evictions": st["evictions"], "bytes_peak_gb": round(st["bytes_peak"] / 1e9, 2),
-                     "bit_identical_to_per_call_on_sample": bool(same_pc), "slowest": slowest})
+                     "bit_identical_to_per_call_on_sample": bool(same_pc), "mismatches": mismatches,
+                     "slowest": slowest})
     clocks = sampler.stop()
     repeats = sum(1 for i, q in enumerate(reqs) if q[3] != i)
     best = max(runs, key=lambda x: x["solves_per_s"])

@@ -30,6 +30,16 @@ namespace pg {
 // ---------------------------------------------------------------------------
 // LU panel
 // ---------------------------------------------------------------------------
+// Two launches per panel column k, synchronised only by the kernel boundary:
+//   lu_update_kernel  blocks over (rows > k) x (groups of PANEL_CG columns in (k, jb)):
+//                     l_i = a_ik scaled as Rgetrf2 does, a_ic += (-u_kc)*l_i.  Column k is
+//                     only read; the first column group writes l_i to a scratch column.
+//   lu_pivot_kernel   one block: the scratch column into column k, then the pivot step of
+//                     column k+1 -- iRamax over the updated column, the interchange of the
+//                     pivot row across the panel, the scaling decision.
+constexpr int PANEL_ROWS = 128; // rows per update block (one per thread)
+constexpr int PANEL_CG = 4;     // panel columns per update block
+
 // Pivot decision of one column, shared by the two kernels of a panel step.
 struct PivotInfo {
     int row;       // panel-local row of the pivot
@@ -38,18 +48,34 @@ struct PivotInfo {
     uint32_t recip;
 };
 
-// iRamax (iRamax.cpp:65-71) over panel-local rows [k, M) of column k: the first index of
+// Workspace of the panel kernels: the pivot/diagonal record and a scratch column of m
+// entries, then the trailing GEMM's workspace.
+static size_t panel_ws_bytes(int m) { return 256 + (((size_t)m * 4 + 255) & ~(size_t)255); }
+
+// Copies the scaled multipliers of column `copy_col` (rows copy_col+1 .. M-1) from the
+// scratch column into place (copy_col < 0: none), then, when k < jb, the pivot step of
+// column k: iRamax (iRamax.cpp:65-71) over panel-local rows [k, M) -- the first index of
 // the strict maximum of abs() in posit order (signed integer order of the patterns, NaR
-// lowest), then the interchange of rows k and p over the panel's jb columns
+// lowest) -- the interchange of rows k and p over the panel's jb columns
 // (Rgetrf2.cpp:107-117) and the scaling decision (Rgetrf2.cpp:119-131).
-__global__ void lu_pivot_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k, int row0,
-                                int *__restrict__ ipiv, int *__restrict__ info, PivotInfo *__restrict__ pinfo)
+__global__ void __launch_bounds__(1024) lu_pivot_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
+                                                        int row0, int *__restrict__ ipiv, int *__restrict__ info,
+                                                        PivotInfo *__restrict__ pinfo,
+                                                        const uint32_t *__restrict__ lcol, int copy_col)
 {
     __shared__ int32_t s_key[1024];
     __shared__ int s_idx[1024];
     if (*info < 0)
         return; // an earlier failure stops the factorization
     const int tid = threadIdx.x;
+    if (copy_col >= 0) {
+        uint32_t *pc = P + (size_t)copy_col * lda;
+        for (int r = copy_col + 1 + tid; r < M; r += blockDim.x)
+            pc[r] = lcol[r];
+        __syncthreads(); // the interchange below moves two of these entries
+    }
+    if (k >= jb)
+        return;
     int32_t best = INT32_MIN;
     int bidx = -1;
     const uint32_t *col = P + (size_t)k * lda;
@@ -107,32 +133,38 @@ __global__ void lu_pivot_kernel(uint32_t *__restrict__ P, size_t lda, int M, int
     }
 }
 
-// Scale column k below the pivot and apply the rank-1 update to panel columns k+1..jb-1
-// for rows k+1..M-1.  Each thread owns one row; the pivot row (row k, after the
-// interchange) is staged in shared memory.
-__global__ void lu_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
-                                 const int *__restrict__ info, const PivotInfo *__restrict__ pinfo)
+PG_HD uint32_t lu_scaled(uint32_t a, const PivotInfo &pi)
 {
-    extern __shared__ uint32_t s_u[]; // -u_kc for c in (k, jb)
+    if (pi.mode == 1)
+        return pmul(pi.recip, a); // Rscal: da*dx
+    if (pi.mode == 2)
+        return pdiv(a, pi.piv);
+    return a;
+}
+
+__global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb,
+                                                               int k, const int *__restrict__ info,
+                                                               const PivotInfo *__restrict__ pinfo,
+                                                               uint32_t *__restrict__ lcol)
+{
+    __shared__ uint32_t s_u[PANEL_CG]; // -u_kc for this block's columns
     if (*info < 0)
         return;
     const PivotInfo pi = *pinfo;
-    for (int c = k + 1 + threadIdx.x; c < jb; c += blockDim.x)
-        s_u[c - k - 1] = pneg(P[k + (size_t)c * lda]);
+    const int c0 = k + 1 + blockIdx.y * PANEL_CG;
+    if (threadIdx.x < PANEL_CG && c0 + (int)threadIdx.x < jb)
+        s_u[threadIdx.x] = pneg(P[k + (size_t)(c0 + threadIdx.x) * lda]); // row k after the interchange
     __syncthreads();
-    const int i = k + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = k + 1 + blockIdx.x * PANEL_ROWS + threadIdx.x;
     if (i >= M)
         return;
-    uint32_t *pk = P + (size_t)k * lda;
-    uint32_t l = pk[i];
-    if (pi.mode == 1)
-        l = pmul(pi.recip, l); // Rscal: da*dx
-    else if (pi.mode == 2)
-        l = pdiv(l, pi.piv);
-    pk[i] = l;
-    for (int c = k + 1; c < jb; ++c) {
-        uint32_t *pc = P + (size_t)c * lda + i;
-        *pc = padd(*pc, pmul(s_u[c - k - 1], l));
+    const uint32_t l = lu_scaled(P[i + (size_t)k * lda], pi);
+    if (blockIdx.y == 0)
+        lcol[i] = l;
+    const int cn = min(PANEL_CG, jb - c0);
+    for (int j = 0; j < cn; ++j) {
+        uint32_t *pc = P + i + (size_t)(c0 + j) * lda;
+        *pc = padd(*pc, pmul(s_u[j], l));
     }
 }
 
@@ -325,18 +357,34 @@ size_t llt_pc_smem_bytes(int m) { return (size_t)m * (2 * sizeof(PackedDp) + 4);
 // ---------------------------------------------------------------------------
 // Cholesky panel (lower)
 // ---------------------------------------------------------------------------
-// Step k of the panel whose top-left corner is the diagonal entry (row0, row0), in two
-// kernels.  chol_diag_kernel (one CTA): l_kk = sqrt(a_kk) -- a_kk <= 0 in posit order, NaR
-// included, stops with info (Rpotrf2.cpp:90-93) -- and l_ck = (1/l_kk)*a_ck for the rows
-// c in (k, jb) of the panel's diagonal block (Rtrsm.cpp:265-268).  chol_update_kernel:
-// l_ik = (1/l_kk)*a_ik for the rows below the diagonal block, then the rank-1 update of
-// the panel's lower part, a_ic += (-l_ck)*l_ik for k < c <= i, rows in parallel.
-__global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int jb, int k, int row0,
-                                 int *__restrict__ info, uint32_t *__restrict__ recip_out)
+// Two launches per panel column k, as for LU:
+//   chol_update_kernel  blocks over (rows > k) x (column groups in (k, jb)): l_ik =
+//                       (1/l_kk)*a_ik for the rows below the diagonal block (those of the
+//                       block were scaled by the diagonal step; Rtrsm.cpp:265-268), then
+//                       a_ic += (-l_ck)*l_ik for k < c <= i.  Column k is only read; the
+//                       first column group writes the new l_ik to a scratch column.
+//   chol_diag_kernel    one block: the scratch column into column k, then the diagonal step
+//                       of column k+1: l_kk = sqrt(a_kk) -- a_kk <= 0 in posit order, NaR
+//                       included, stops with info (Rpotrf2.cpp:90-93) -- and
+//                       l_ck = (1/l_kk)*a_ck for the rows c in (k, jb).
+struct CholSync {
+    uint32_t recip; // 1/l_kk of the current column
+};
+
+__global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k, int row0,
+                                 int *__restrict__ info, CholSync *__restrict__ sync,
+                                 const uint32_t *__restrict__ lcol, int copy_col)
 {
     __shared__ uint32_t s_recip;
     __shared__ int s_stop;
     if (*info != 0)
+        return;
+    if (copy_col >= 0) {
+        uint32_t *pc = P + (size_t)copy_col * lda;
+        for (int r = (copy_col + 1 > jb ? copy_col + 1 : jb) + threadIdx.x; r < M; r += blockDim.x)
+            pc[r] = lcol[r];
+    }
+    if (k >= jb)
         return;
     uint32_t *pk = P + (size_t)k * lda;
     if (threadIdx.x == 0) {
@@ -348,7 +396,7 @@ __global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int jb, i
             uint32_t lkk = psqrt(akk);
             s_recip = pdiv(P32_ONE, lkk);
             pk[k] = lkk;
-            *recip_out = s_recip;
+            sync->recip = s_recip;
         }
     }
     __syncthreads();
@@ -358,28 +406,31 @@ __global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int jb, i
         pk[c] = pmul(s_recip, pk[c]);
 }
 
-__global__ void chol_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
-                                   const int *__restrict__ info, const uint32_t *__restrict__ recip_in)
+__global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__restrict__ P, size_t lda, int M,
+                                                                 int jb, int k, const int *__restrict__ info,
+                                                                 const CholSync *__restrict__ sync,
+                                                                 uint32_t *__restrict__ lcol)
 {
-    extern __shared__ uint32_t s_l[]; // -l_ck for c in (k, jb)
+    __shared__ uint32_t s_l[PANEL_CG]; // -l_ck for this block's columns
     if (*info != 0)
         return;
+    const uint32_t recip = sync->recip;
     const uint32_t *pk = P + (size_t)k * lda;
-    for (int c = k + 1 + threadIdx.x; c < jb; c += blockDim.x)
-        s_l[c - k - 1] = pneg(pk[c]);
+    const int c0 = k + 1 + blockIdx.y * PANEL_CG;
+    if (threadIdx.x < PANEL_CG && c0 + (int)threadIdx.x < jb)
+        s_l[threadIdx.x] = pneg(pk[c0 + threadIdx.x]); // scaled by the diagonal step
     __syncthreads();
-    const int i = k + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = k + 1 + blockIdx.x * PANEL_ROWS + threadIdx.x;
     if (i >= M)
         return;
-    uint32_t l = pk[i];
-    if (i >= jb) { // rows of the diagonal block were scaled by chol_diag_kernel
-        l = pmul(*recip_in, l);
-        P[(size_t)k * lda + i] = l;
-    }
-    const int cmax = min(jb - 1, i);
-    for (int c = k + 1; c <= cmax; ++c) {
-        uint32_t *pc = P + (size_t)c * lda + i;
-        *pc = padd(*pc, pmul(s_l[c - k - 1], l));
+    const uint32_t a = pk[i];
+    const uint32_t l = i >= jb ? pmul(recip, a) : a;
+    if (blockIdx.y == 0 && i >= jb)
+        lcol[i] = l;
+    const int cn = min(min(PANEL_CG, jb - c0), i - c0 + 1);
+    for (int j = 0; j < cn; ++j) {
+        uint32_t *pc = P + i + (size_t)(c0 + j) * lda;
+        *pc = padd(*pc, pmul(s_l[j], l));
     }
 }
 
@@ -387,6 +438,7 @@ __global__ void chol_update_kernel(uint32_t *__restrict__ P, size_t lda, int M, 
 // Host orchestration
 // ---------------------------------------------------------------------------
 static int imin(int a, int b) { return a < b ? a : b; }
+static int imax(int a, int b) { return a > b ? a : b; }
 
 size_t rgetrf_workspace_bytes(int m, int n, int nb)
 {
@@ -395,11 +447,17 @@ size_t rgetrf_workspace_bytes(int m, int n, int nb)
         nb = 1;
     int jb = imin(nb, mn);
     size_t g = mn > jb ? gemm_workspace_bytes(m - jb > 0 ? m - jb : 1, n - jb > 0 ? n - jb : 1, jb) : 0;
-    return 256 + g;
+    return panel_ws_bytes(m) + g;
 }
 
-// Rgetrf.cpp:95-132 with the device kernels above.  `ws` holds a PivotInfo and the
-// trailing GEMM's workspace.
+static dim3 panel_grid(int M, int jb, int k)
+{
+    return dim3((unsigned)imax((M - k - 1 + PANEL_ROWS - 1) / PANEL_ROWS, 1),
+                (unsigned)imax((jb - k - 1 + PANEL_CG - 1) / PANEL_CG, 1));
+}
+
+// Rgetrf.cpp:95-132 with the device kernels above.  `ws` holds the pivot record, the
+// scratch column and the trailing GEMM's workspace.
 cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *ws,
                           cudaStream_t st)
 {
@@ -407,19 +465,18 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
     if (nb < 1)
         nb = 1;
     PivotInfo *pinfo = reinterpret_cast<PivotInfo *>(ws);
-    void *gws = reinterpret_cast<unsigned char *>(ws) + 256;
+    uint32_t *lcol = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(ws) + 256);
+    void *gws = reinterpret_cast<unsigned char *>(ws) + panel_ws_bytes(m);
     const size_t L = (size_t)lda;
     for (int j = 0; j < mn; j += nb) {
         const int jb = imin(mn - j, nb);
         const int M = m - j;
         uint32_t *P = A + j + (size_t)j * L;
+        uint32_t *lc = lcol + j; // indexed by panel-local row
+        lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, 0, j, ipiv, info, pinfo, lc, -1);
         for (int k = 0; k < jb; ++k) {
-            lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k, j, ipiv, info, pinfo);
-            const int rows = M - k - 1;
-            if (rows > 0 || k + 1 < jb) {
-                const int blocks = rows > 0 ? (rows + 255) / 256 : 1;
-                lu_update_kernel<<<blocks, 256, (size_t)jb * 4, st>>>(P, L, M, jb, k, info, pinfo);
-            }
+            lu_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, pinfo, lc);
+            lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k + 1, j, ipiv, info, pinfo, lc, k);
         }
         if (j > 0)
             laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
@@ -446,7 +503,7 @@ size_t rpotrf_workspace_bytes(int n, int nb)
     if (nb < 1)
         nb = 1;
     int jb = imin(nb, n);
-    return 256 + (n > jb ? gemm_workspace_bytes(n - jb, n - jb, jb) : 0);
+    return panel_ws_bytes(n) + (n > jb ? gemm_workspace_bytes(n - jb, n - jb, jb) : 0);
 }
 
 // Lower Cholesky (Rpotrf.cpp:124-142 / Rpotrf2.cpp:132-146 order, blocked right-looking).
@@ -454,20 +511,19 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
 {
     if (nb < 1)
         nb = 1;
-    void *gws = reinterpret_cast<unsigned char *>(ws) + 256;
+    CholSync *sync = reinterpret_cast<CholSync *>(ws);
+    uint32_t *lcol = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(ws) + 256);
+    void *gws = reinterpret_cast<unsigned char *>(ws) + panel_ws_bytes(n);
     const size_t L = (size_t)lda;
     for (int j = 0; j < n; j += nb) {
         const int jb = imin(n - j, nb);
         const int M = n - j;
         uint32_t *P = A + j + (size_t)j * L;
-        uint32_t *recip = reinterpret_cast<uint32_t *>(ws);
+        uint32_t *lc = lcol + j;
+        chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, 0, j, info, sync, lc, -1);
         for (int k = 0; k < jb; ++k) {
-            chol_diag_kernel<<<1, 256, 0, st>>>(P, L, jb, k, j, info, recip);
-            const int rows = M - k - 1;
-            if (rows > 0) {
-                const int blocks = (rows + 255) / 256;
-                chol_update_kernel<<<blocks, 256, (size_t)jb * 4, st>>>(P, L, M, jb, k, info, recip);
-            }
+            chol_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, sync, lc);
+            chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, k + 1, j, info, sync, lc, k);
         }
         if (j + jb < n) {
             const int nr = n - j - jb;
