@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--gemms", type=int, default=50000, help="batch: GEMM problems")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests per arrival rate")
     ap.add_argument("--rates", default="5,10,20,40,burst", help="serve: Poisson arrival rates (req/s)")
-    ap.add_argument("--per-call-sample", type=int, default=100, help="serve: requests timed on the per-call path")
+    ap.add_argument("--per-call-sample", type=int, default=0,
+                    help="serve: requests timed on the per-call path (0: all of them)")
     ap.add_argument("--batch-max-n", type=int, default=0, help="serve: batched-kernel size limit (0: default)")
     ap.add_argument("--lanes", type=int, default=0, help="serve: CUDA streams of the server (0: default)")
     ap.add_argument("--launch-threads", type=int, default=0, help="serve: launcher threads (0: default)")
@@ -640,7 +641,7 @@ def serve_arm(args):
     zeros = lambda i: torch.zeros(reqs[i][1] * reqs[i][2], dtype=torch.int32, pin_memory=True)
 
     # plain per-call path, one request after another
-    S = min(R, args.per_call_sample)
+    S = min(R, args.per_call_sample) if args.per_call_sample > 0 else R
     fac_src = {m: mats[m].numpy().view(np.uint32).copy() for (_, _, _, m) in reqs[:S]}
     xs = [rhs[i].numpy().view(np.uint32).copy() for i in range(S)]
     pc_info, factors, pc_lat = [], {}, []

@@ -182,8 +182,8 @@ typedef struct {
     size_t memory_budget; /* device bytes; 0 = 150 GB (capped at free memory - 2 GiB) */
     int max_inflight;     /* admitted, unfinished requests; 0 = 4096 */
     int max_queue;        /* submitted, not yet admitted requests; 0 = 2^20 */
-    int lanes;            /* CUDA streams work units run on; 0 = 32 */
-    int launch_threads;   /* threads issuing the units' CUDA work; 0 = 4 */
+    int lanes;            /* CUDA streams work units run on; 0 = 64 */
+    int launch_threads;   /* threads issuing the units' CUDA work; 0 = 8 */
     int batch_max_n;      /* n <= this goes to the batched kernel; 0 = 256 (max POSIT_BATCH_MAX_N) */
     int nb;               /* panel width of the blocked path; 0 = 64 */
     int cache_off;        /* 1: never keep factors */

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
                                                                      bool unit, const int *__restrict__ info)
 {
     extern __shared__ __align__(16) unsigned char smem_pc[];
-    PackedDp *s_q = reinterpret_cast<PackedDp *>(smem_pc); // [2][m]
+    double *s_q = reinterpret_cast<double *>(smem_pc); // [2][m]: terms, FP64
     uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
     __shared__ uint32_t s_nar[2];
     if (info && *info < 0)
@@ -325,13 +325,13 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
             const uint32_t *li = L + (size_t)i * ldl;
             const uint32_t bi = s_b[i];
             uint32_t nar = (bi == P32_NAR) | s_nar[cur];
-            dp32 c = decode_gemm(bi == P32_NAR ? 0u : bi);
+            double c = p32_to_double(bi == P32_NAR ? 0u : bi);
             if (i + 1 < m) {
-                const PackedDp q0 = llt_term(li[i + 1], s_b[i + 1], &nar);
+                const double q0 = llt_term(li[i + 1], s_b[i + 1], &nar);
                 c = chain_add_run(c, &q0, 1);
                 c = chain_add_run(c, s_q + (size_t)cur * m + (i + 2), m - i - 2);
             }
-            uint32_t t = nar ? P32_NAR : encode(c);
+            uint32_t t = nar ? P32_NAR : p32_from_double(c);
             if (!unit)
                 t = pdiv(t, li[i]);
             s_b[i] = t;
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
         } else if (tid >= 32 && i >= 1) {
             // terms k = i+1 .. m-1 of row i-1 (their b_k are final)
             const uint32_t *lp = L + (size_t)(i - 1) * ldl;
-            PackedDp *qn = s_q + (size_t)(cur ^ 1) * m;
+            double *qn = s_q + (size_t)(cur ^ 1) * m;
             uint32_t nar = 0;
             for (int k = i + 1 + (tid - 32); k < m; k += LLT_PC_THREADS - 32)
                 qn[k] = llt_term(lp[k], s_b[k], &nar);
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
         bcol[k] = s_b[k];
 }
 
-size_t llt_pc_smem_bytes(int m) { return (size_t)m * (2 * sizeof(PackedDp) + 4); }
+size_t llt_pc_smem_bytes(int m) { return (size_t)m * (2 * sizeof(double) + 4); }
 
 // ---------------------------------------------------------------------------
 // Cholesky panel (lower)

@@ -712,9 +712,9 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
     s->batch_max_n = c.batch_max_n > 0 ? std::min(c.batch_max_n, POSIT_BATCH_MAX_N) : 256;
     s->nb = c.nb > 0 ? c.nb : 64;
     s->cache_on = c.cache_off == 0;
-    const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 32);
+    const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 64);
     const int nbatch = std::min(nlanes - 1, c.batch_lanes > 0 ? c.batch_lanes : 4);
-    const int nlaunch = c.launch_threads > 0 ? c.launch_threads : 4;
+    const int nlaunch = c.launch_threads > 0 ? c.launch_threads : 8;
 
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;

@@ -91,65 +91,107 @@ PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, in
 }
 
 // ---------------------------------------------------------------------------
-// Split form: products computed elsewhere, the chain thread only adds.
+// Split form: products computed elsewhere, the chain thread only adds -- in FP64.
 // ---------------------------------------------------------------------------
-// A decoded posit packed in 8 bytes (one shared-memory load): {scale, significand | sign<<31}.
-struct alignas(8) PackedDp {
-    int32_t s;
-    uint32_t gx;
-};
-PG_HD PackedDp pack_q(const dp32 &d) { return PackedDp{d.s, d.g | (d.x << 31)}; }
-PG_HD dp32 unpack_q(const PackedDp &p)
+// A posit32 value is exact in FP64 (at most 28 significant bits, scale within +-120).
+// One step t + q of the chain is then:
+//   s = fl64(t + q)        exact whenever the operands' binades are at most 24 apart
+//                          (the sum needs at most 29 + 24 bits);
+//   r = (s + C) - C        C = 1.5 * 2^(e + 52 - fb), e the binade of s and fb the posit's
+//                          fraction width there: round to nearest even at the posit's last
+//                          fraction bit (ties to the even pattern, whose parity is the
+//                          fraction's).
+// The reference's p32_add is that rounding of the exact sum (within its 64-bit frame; an
+// addend more than 30 binades down contributes nothing, which is also what rounding the
+// exact sum gives).  More than 30 binades apart, fl64(t + q) may be inexact but lies far
+// from every rounding boundary, so r is still right.  A step is handed to the exact path
+// when the operands are 25..30 binades apart (the FP64 rounding could meet a posit tie),
+// or when the sum's scale is outside the fast window (regime longer than 27 bits, fewer
+// than one fraction bit; this includes an exactly cancelling sum, whose FP64 value is 0).
+// The dependent path per step: three FP64 additions and a handful of integer operations
+// that build C from the exponent of s.
+PG_HD uint64_t f64_bits(double x)
 {
-    dp32 d;
-    d.s = p.s;
-    d.g = p.gx & 0x7FFFFFFFu;
-    d.x = p.gx >> 31;
-    return d;
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+}
+PG_HD double f64_from_bits(uint64_t b)
+{
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+}
+PG_HD double f64_add(double a, double b)
+{
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(a, b); // never contracted or reassociated
+#else
+    return a + b;
+#endif
+}
+
+// t + q rounded to posit32, both posit values held in FP64; bit 30 of `bad` is set when
+// the step must come from the exact path instead.
+PG_HD double f64_posit_add(double t, double q, uint32_t &bad)
+{
+    const double s = f64_add(t, q);
+    const int32_t eb = (int32_t)((f64_bits(s) >> 52) & 0x7FF); // biased binade of s
+    const int32_t k = (eb - 1023) >> 2;                         // regime value
+    const int32_t run = (k ^ (k >> 31)) + 1;                     // regime run; fb = 28 - run
+    const uint32_t hc = ((uint32_t)(eb + 24 + run) << 20) | 0x00080000u; // 1.5 * 2^(e - fb + 52)
+    const double C = f64_from_bits((uint64_t)hc << 32);
+    const double r = f64_add(f64_add(s, C), -C);
+    // off the dependent path: is this step one the FP64 form does exactly?
+    const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
+    const int32_t gap = et > eq ? et - eq : eq - et;
+    const bool risky = (et != 0) & (eq != 0) & (gap > 24) & (gap <= 30);
+    const bool outside = (uint32_t)(eb - 1023 - FAST_LO) > (uint32_t)(FAST_HI - FAST_LO);
+    bad |= (risky | outside) ? 0x40000000u : 0u;
+    return r;
+}
+
+// The exact step on patterns (rare).
+PG_HD_NOINLINE double f64_posit_add_exact(double t, double q)
+{
+    return p32_to_double(padd(p32_from_double(t), p32_from_double(q)));
 }
 
 // The term -a_ki*b_k of the dot-form solve as the reference rounds it (p32_mul,
-// kernel_entry.cl:399-538), decoded; *nar is set when it is NaR.
-PG_HD PackedDp llt_term(uint32_t l, uint32_t bk, uint32_t *nar)
+// kernel_entry.cl:399-538), in FP64; *nar is set when it is NaR (the term is then 0).
+PG_HD double llt_term(uint32_t l, uint32_t bk, uint32_t *nar)
 {
     const uint32_t p = pmul(0u - bk, l); // (-b)*a == -(a*b) bit for bit
     *nar |= p == P32_NAR;
-    return pack_q(decode_gemm(p == P32_NAR ? 0u : p));
+    return p32_to_double(p == P32_NAR ? 0u : p);
 }
 
-PG_HD_NOINLINE dp32 dadd_exact(dp32 c, dp32 q) { return decode_gemm(padd(encode(c), encode(q))); }
-
-// c + q_0 + q_1 + ... + q_{count-1}, every addition rounded (p32_add), in that order; the
-// q are decoded posit32 values.  Blocks of CHAIN_BLOCK additions without a branch, the
-// failure flags tested per block, a flagged block replayed exactly.
-PG_HD dp32 chain_add_run(dp32 c, const PackedDp *q, int count)
+// t + q_0 + q_1 + ... + q_{count-1}, every addition rounded (p32_add), in that order; t
+// and the q are posit32 values in FP64.  Blocks of CHAIN_BLOCK steps without a branch, the
+// flags tested once per block, a flagged block replayed exactly from its start.
+PG_HD double chain_add_run(double t, const double *q, int count)
 {
     constexpr int U = CHAIN_BLOCK;
     int k = 0;
     if (count >= U) {
-        PackedDp v[U];
+        double v[U];
 #pragma unroll
         for (int j = 0; j < U; ++j)
             v[j] = q[j];
         for (; k + U <= count; k += U) {
-            PackedDp nv[U];
+            double nv[U];
 #pragma unroll
             for (int j = 0; j < U; ++j)
                 nv[j] = q[k + U + j < count ? k + U + j : count - 1];
-            const dp32 c0 = c;
+            const double t0 = t;
             uint32_t bad = 0;
 #pragma unroll
-            for (int j = 0; j < U; ++j) {
-                dp32 r;
-                uint32_t ba;
-                dadd_core(c, unpack_q(v[j]), ComputedEntry{}, r, ba);
-                c = r;
-                bad |= ba;
-            }
+            for (int j = 0; j < U; ++j)
+                t = f64_posit_add(t, v[j], bad);
             if (bad & 0x40000000u) {
-                c = c0;
+                t = t0;
                 for (int j = 0; j < U; ++j)
-                    c = dadd_exact(c, unpack_q(v[j]));
+                    t = f64_posit_add_exact(t, v[j]);
             }
 #pragma unroll
             for (int j = 0; j < U; ++j)
@@ -157,13 +199,11 @@ PG_HD dp32 chain_add_run(dp32 c, const PackedDp *q, int count)
         }
     }
     for (; k < count; ++k) {
-        const dp32 qk = unpack_q(q[k]);
-        dp32 r;
-        uint32_t ba;
-        dadd_core(c, qk, ComputedEntry{}, r, ba);
-        c = (ba & 0x40000000u) ? dadd_exact(c, qk) : r;
+        uint32_t bad = 0;
+        const double r = f64_posit_add(t, q[k], bad);
+        t = (bad & 0x40000000u) ? f64_posit_add_exact(t, q[k]) : r;
     }
-    return c;
+    return t;
 }
 
 } // namespace pg

@@ -81,18 +81,18 @@ long hc_decode_bf_mismatch(const uint32_t *u, long n)
 // the split L^T solve (products as llt_term, additions as chain_add_run), row by row
 void hc_llt_solve_split(const uint32_t *L, long ld, uint32_t *b, int m)
 {
-    PackedDp *q = new PackedDp[m > 0 ? m : 1];
+    double *q = new double[m > 0 ? m : 1];
     for (int i = m - 1; i >= 0; --i) {
         const uint32_t *li = L + (long)i * ld;
         uint32_t nar = b[i] == P32_NAR;
         for (int k = i + 1; k < m; ++k)
             q[k] = llt_term(li[k], b[k], &nar);
-        dp32 c = decode_gemm(b[i] == P32_NAR ? 0u : b[i]);
+        double c = p32_to_double(b[i] == P32_NAR ? 0u : b[i]);
         if (i + 1 < m) {
             c = chain_add_run(c, q + i + 1, 1);
             c = chain_add_run(c, q + i + 2, m - i - 2);
         }
-        uint32_t t = nar ? P32_NAR : encode(c);
+        uint32_t t = nar ? P32_NAR : p32_from_double(c);
         b[i] = pdiv(t, li[i]);
     }
     delete[] q;
@@ -100,11 +100,24 @@ void hc_llt_solve_split(const uint32_t *L, long ld, uint32_t *b, int m)
 // chain_add_run over n terms from patterns (NaR excluded by the caller)
 uint32_t hc_chain_add(uint32_t c0, const uint32_t *q, int n)
 {
-    PackedDp *d = new PackedDp[n > 0 ? n : 1];
+    double *d = new double[n > 0 ? n : 1];
     for (int k = 0; k < n; ++k)
-        d[k] = pack_q(decode_gemm(q[k]));
-    uint32_t r = encode(chain_add_run(decode_gemm(c0), d, n));
+        d[k] = p32_to_double(q[k]);
+    uint32_t r = p32_from_double(chain_add_run(p32_to_double(c0), d, n));
     delete[] d;
     return r;
+}
+// single FP64 chain steps t + q (with their exact fallback) on n pairs; returns the number
+// of steps the FP64 form handed to the exact path
+long hc_f64_add_n(const uint32_t *t, const uint32_t *q, uint32_t *o, long n)
+{
+    long flagged = 0;
+    for (long i = 0; i < n; i++) {
+        uint32_t bad = 0;
+        const double r = f64_posit_add(p32_to_double(t[i]), p32_to_double(q[i]), bad);
+        flagged += (bad & 0x40000000u) != 0;
+        o[i] = p32_from_double((bad & 0x40000000u) ? f64_posit_add_exact(p32_to_double(t[i]), p32_to_double(q[i])) : r);
+    }
+    return flagged;
 }
 }

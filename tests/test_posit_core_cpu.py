@@ -33,6 +33,8 @@ def hc(tmp_path_factory):
     lib.hc_llt_solve_split.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
     lib.hc_chain_add.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.restype = ctypes.c_uint32
+    lib.hc_f64_add_n.argtypes = [U32, U32, U32, ctypes.c_long]
+    lib.hc_f64_add_n.restype = ctypes.c_long
     lib.hc_decode_bf_mismatch.argtypes = [U32, ctypes.c_long]
     lib.hc_decode_bf_mismatch.restype = ctypes.c_long
     return lib
@@ -177,4 +179,29 @@ def test_chain_of_additions_matches_oracle(hc):
         for k in range(n):
             oracle.orc.orc_p32_add_n(want, q[k:k + 1].copy(), want, 1)
         assert hc.hc_chain_add(c0, np.ascontiguousarray(q), n) == int(want[0]), (trial, n)
+
+
+def test_fp64_chain_step_matches_oracle_across_binade_gaps(hc):
+    """The FP64 step of the triangular-solve chain (add in FP64, round to the posit's
+    fraction width with a magic constant, hand risky steps to the exact path) equals
+    p32_add for operand gaps of 0..40 binades -- the exact, the risky (25..30) and the
+    absorbed (> 30) ranges -- near-ties, cancellations, zeros and the regime extremes."""
+    rng = np.random.default_rng(21)
+    n = 300_000
+    base = rng.uniform(-30, 30, n)
+    gap = rng.integers(0, 41, n)
+    t = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 2.0 ** base * rng.uniform(1, 2, n))
+    q = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 2.0 ** (base - gap) * rng.uniform(1, 2, n))
+    # near-ties: q just around half an ulp of t (t's last fraction bits flipped by q)
+    tie = oracle.to_double(t[:50_000])
+    q[:50_000] = oracle.from_double(tie * 2.0 ** -28 * rng.choice([1.0, -1.0, 0.999999, 1.000001], 50_000))
+    q[50_000:60_000] = (0 - t[50_000:60_000].astype(np.uint64)).astype(np.uint32)  # exact cancellation
+    q[60_000:62_000] = 0
+    t[62_000:64_000] = oracle.from_double(np.sign(rng.uniform(-1, 1, 2000)) * 2.0 ** rng.uniform(95, 118, 2000))
+    out = np.empty_like(t)
+    flagged = hc.hc_f64_add_n(t, q, out, n)
+    want = np.empty_like(t)
+    oracle.orc.orc_p32_add_n(t, q, want, n)
+    assert np.array_equal(out, want)
+    assert 0 < flagged < n // 2  # near-ties sit in the risky 25..30-binade band by design
 
