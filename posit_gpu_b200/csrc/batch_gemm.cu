@@ -22,8 +22,8 @@ constexpr int BG_THREADS = 256;
 constexpr int BG_MAXB = 64; // largest tile side
 
 template <int TM_, int TN_>
-__device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, uint2 *Ts, unsigned char *rnar,
-                           unsigned char *cnar, const RegimeEntry *tbl)
+__device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, double *As, double *Ts, unsigned char *rnar,
+                           unsigned char *cnar, const uint64_t *ctab)
 {
     constexpr int BM_ = 16 * TM_, BN_ = 16 * TN_;
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
@@ -33,7 +33,7 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, ui
         rnar[i] = 0;
     for (int j = tid; j < BN_; j += BG_THREADS)
         cnar[j] = 0;
-    dp32 acc[TM_][TN_];
+    double acc[TM_][TN_];
     uint32_t nar_bits = 0;
 #pragma unroll
     for (int i = 0; i < TM_; ++i) {
@@ -55,7 +55,7 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, ui
                     u = P32_ONE;
                 }
             }
-            acc[i][j] = decode_gemm(u);
+            acc[i][j] = p32_to_double(u);
         }
     }
     __syncthreads();
@@ -71,7 +71,7 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, ui
                 rnar[i] = 1;
                 u = P32_ONE;
             }
-            As[l * BM_ + i] = pack_dp(decode_gemm(u));
+            As[l * BM_ + i] = p32_to_double(u);
         }
         for (int e = tid; e < BK * BN_; e += BG_THREADS) {
             const int j = e % BN_, l = e / BN_;
@@ -86,10 +86,10 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, ui
                 cnar[j] = 1;
                 u = P32_ONE;
             }
-            Ts[l * BN_ + j] = pack_dp(decode_gemm(u));
+            Ts[l * BN_ + j] = p32_to_double(u);
         }
         __syncthreads();
-        tile_steps<TM_, TN_>(acc, As, Ts, min(BK, k - kt * BK), tbl, tx, ty);
+        tile_steps_f64<TM_, TN_>(acc, As, Ts, min(BK, k - kt * BK), ctab, tx, ty);
         __syncthreads();
     }
 #pragma unroll
@@ -101,7 +101,7 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, uint2 *As, ui
             if (row < m && col < n) {
                 uint32_t *cp = P.C + (size_t)row + (size_t)col * P.ldc;
                 const bool nar = ((nar_bits >> (i * TN_ + j)) & 1u) || rnar[li] || cnar[lj];
-                uint32_t v = nar ? P32_NAR : encode(acc[i][j]);
+                uint32_t v = nar ? P32_NAR : p32_from_double(acc[i][j]);
                 if (dot) {
                     uint32_t at = pmul(P.alpha, v);
                     v = (P.beta == 0) ? at : padd(at, pmul(P.beta, *cp));
@@ -131,15 +131,14 @@ __global__ void __launch_bounds__(BG_THREADS, 2)
                       int *__restrict__ next)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    RegimeEntry *rtab = reinterpret_cast<RegimeEntry *>(smem);
-    uint2 *As = reinterpret_cast<uint2 *>(smem + (size_t)RT_N * sizeof(RegimeEntry));
-    uint2 *Ts = As + BK * BG_MAXB;
+    uint64_t *ctab = reinterpret_cast<uint64_t *>(smem); // rounding constant per FP64 binade
+    double *As = reinterpret_cast<double *>(smem + (size_t)F64_BINADES * sizeof(uint64_t));
+    double *Ts = As + BK * BG_MAXB;
     unsigned char *rnar = reinterpret_cast<unsigned char *>(Ts + BK * BG_MAXB);
     unsigned char *cnar = rnar + BG_MAXB;
     __shared__ int s_item;
-    for (int i = threadIdx.x; i < RT_N; i += BG_THREADS)
-        rtab[i] = regime_entry(RT_MIN + i);
-    const RegimeEntry *tbl = rtab - RT_MIN;
+    for (int i = threadIdx.x; i < F64_BINADES; i += BG_THREADS)
+        ctab[i] = f64_round_const(i);
     __syncthreads();
     for (;;) {
         if (threadIdx.x == 0)
@@ -155,18 +154,18 @@ __global__ void __launch_bounds__(BG_THREADS, 2)
         if (P.alpha == 0 || P.k == 0)
             batch_scale_tile(P, t.mt, t.nt, bm, bn);
         else if (t.cfg == 0)
-            batch_tile<4, 2>(P, t.mt, t.nt, As, Ts, rnar, cnar, tbl);
+            batch_tile<4, 2>(P, t.mt, t.nt, As, Ts, rnar, cnar, ctab);
         else if (t.cfg == 1)
-            batch_tile<2, 2>(P, t.mt, t.nt, As, Ts, rnar, cnar, tbl);
+            batch_tile<2, 2>(P, t.mt, t.nt, As, Ts, rnar, cnar, ctab);
         else
-            batch_tile<2, 4>(P, t.mt, t.nt, As, Ts, rnar, cnar, tbl);
+            batch_tile<2, 4>(P, t.mt, t.nt, As, Ts, rnar, cnar, ctab);
         __syncthreads();
     }
 }
 
 size_t batch_gemm_smem_bytes()
 {
-    return (size_t)RT_N * sizeof(RegimeEntry) + 2 * (size_t)BK * BG_MAXB * sizeof(uint2) + 2 * BG_MAXB;
+    return (size_t)F64_BINADES * sizeof(uint64_t) + 2 * (size_t)BK * BG_MAXB * sizeof(double) + 2 * BG_MAXB;
 }
 
 cudaError_t batch_gemm_launch(const BatchGemmDesc *probs, const BatchTile *tiles, int ntiles, int *next, int ctas,

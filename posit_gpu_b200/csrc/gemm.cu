@@ -95,8 +95,8 @@ GemmPlan gemm_plan(int m, int n, int k)
     p.mt = (m + BM - 1) / BM;
     p.nt = (n + BN - 1) / BN;
     p.kt = (k + BK - 1) / BK;
-    p.a_bytes = (size_t)p.mt * p.kt * BK * BM * sizeof(uint2);
-    p.b_bytes = (size_t)p.nt * p.kt * BK * BN * sizeof(uint2);
+    p.a_bytes = (size_t)p.mt * p.kt * BK * BM * sizeof(double);
+    p.b_bytes = (size_t)p.nt * p.kt * BK * BN * sizeof(double);
     p.flag_bytes = (size_t)(p.mt * BM + p.nt * BN);
     return p;
 }
@@ -116,7 +116,7 @@ size_t gemm_workspace_bytes(int m, int n, int k)
 // kernel_entry.cl:385-390, 414-417); that is recorded in row_nar[] and the operand is
 // decoded as 1.0 so the row's arithmetic stays on the fast path.
 __global__ void decode_a_kernel(bool nota, int m, int k, const uint32_t *__restrict__ A, size_t lda,
-                                int KT, size_t total, uint2 *__restrict__ Ad, unsigned char *__restrict__ row_nar)
+                                int KT, size_t total, double *__restrict__ Ad, unsigned char *__restrict__ row_nar)
 {
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
@@ -134,13 +134,13 @@ __global__ void decode_a_kernel(bool nota, int m, int k, const uint32_t *__restr
             row_nar[row] = 1;
             u = P32_ONE;
         }
-        Ad[idx] = pack_dp(decode_gemm(u));
+        Ad[idx] = p32_to_double(u);
     }
 }
 
 // op(B) (k x n) -> Td[nt][kt][l][j], times alpha (exactly rounded) when `scale`.
 __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restrict__ B, size_t ldb,
-                                bool scale, uint32_t alpha, int KT, size_t total, uint2 *__restrict__ Td,
+                                bool scale, uint32_t alpha, int KT, size_t total, double *__restrict__ Td,
                                 unsigned char *__restrict__ col_nar)
 {
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -162,7 +162,7 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
             col_nar[col] = 1;
             u = P32_ONE;
         }
-        Td[idx] = pack_dp(decode_gemm(u));
+        Td[idx] = p32_to_double(u);
     }
 }
 
@@ -176,7 +176,7 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
 template <bool DOT, bool LOWER>
 __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     gemm_main_kernel(int m, int n, int k, int KT, uint32_t alpha, uint32_t beta,
-                     const uint2 *__restrict__ Ad, const uint2 *__restrict__ Td, uint32_t *__restrict__ C,
+                     const double *__restrict__ Ad, const double *__restrict__ Td, uint32_t *__restrict__ C,
                      size_t ldc, const unsigned char *__restrict__ row_nar,
                      const unsigned char *__restrict__ col_nar, const int *__restrict__ stop)
 {
@@ -185,27 +185,26 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     if (LOWER && (int)(blockIdx.x * BM + BM - 1) < (int)(blockIdx.y * BN))
         return; // every row of the tile is above its first column
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint2 *As = reinterpret_cast<uint2 *>(smem_raw);
-    uint2 *Ts = As + STAGES * BK * BM;
-    RegimeEntry *rtab = reinterpret_cast<RegimeEntry *>(Ts + STAGES * BK * BN);
-    const RegimeEntry *tbl = rtab - RT_MIN; // tbl[s] for RT_MIN <= s <= RT_MAX
+    double *As = reinterpret_cast<double *>(smem_raw);
+    double *Ts = As + STAGES * BK * BM;
+    uint64_t *ctab = reinterpret_cast<uint64_t *>(Ts + STAGES * BK * BN); // rounding constant per binade
     __shared__ __align__(8) uint64_t full[STAGES];
 
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
     const int mt = blockIdx.x, nt = blockIdx.y;
-    const uint2 *Ablk = Ad + (size_t)mt * KT * BK * BM;
-    const uint2 *Tblk = Td + (size_t)nt * KT * BK * BN;
-    constexpr uint32_t kATileBytes = BK * BM * sizeof(uint2);
-    constexpr uint32_t kBTileBytes = BK * BN * sizeof(uint2);
+    const double *Ablk = Ad + (size_t)mt * KT * BK * BM;
+    const double *Tblk = Td + (size_t)nt * KT * BK * BN;
+    constexpr uint32_t kATileBytes = BK * BM * sizeof(double);
+    constexpr uint32_t kBTileBytes = BK * BN * sizeof(double);
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s)
             mbar_init(&full[s], 1);
         mbar_fence_init();
     }
-    for (int i = tid; i < RT_N; i += NTHREADS)
-        rtab[i] = regime_entry(RT_MIN + i);
+    for (int i = tid; i < F64_BINADES; i += NTHREADS)
+        ctab[i] = f64_round_const(i);
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < STAGES && s < KT; ++s) {
@@ -217,7 +216,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
 
     // Accumulators: NN/NT start from beta*C, TN/TT from zero.  A NaR start value is
     // remembered in nar_bits (the output stays NaR whatever follows) and replaced by 1.0.
-    dp32 acc[TM][TN];
+    double acc[TM][TN];
     uint32_t nar_bits = 0;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
@@ -239,7 +238,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
                     u = P32_ONE;
                 }
             }
-            acc[i][j] = decode_gemm(u);
+            acc[i][j] = p32_to_double(u);
         }
     }
 
@@ -250,10 +249,10 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
         const int s = kt % STAGES;
         const uint32_t parity = (uint32_t)(kt / STAGES) & 1u;
         const bool arrived = mbar_wait_bounded(&full[s], parity);
-        const uint2 *as = As + s * BK * BM;
-        const uint2 *ts = Ts + s * BK * BN;
+        const double *as = As + s * BK * BM;
+        const double *ts = Ts + s * BK * BN;
         const int lmax = min(BK, k - kt * BK);
-        tile_steps<TM, TN>(acc, as, ts, lmax, tbl, tx, ty);
+        tile_steps_f64<TM, TN>(acc, as, ts, lmax, ctab, tx, ty);
         // every thread is done with stage s before it is refilled
         bad = __syncthreads_or(!arrived) != 0;
         if (bad)
@@ -284,7 +283,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
             if (row < m && col < n && (!LOWER || row >= col)) {
                 uint32_t *cp = C + (size_t)row + (size_t)col * ldc;
                 const bool nar = ((nar_bits >> (i * TN + j)) & 1u) || row_nar[row] || col_nar[col];
-                uint32_t v = nar ? P32_NAR : encode(acc[i][j]);
+                uint32_t v = nar ? P32_NAR : p32_from_double(acc[i][j]);
                 if (DOT) { // Rgemm.cpp:197-201
                     uint32_t at = pmul(alpha, v);
                     v = (beta == 0) ? at : padd(at, pmul(beta, *cp));
@@ -394,19 +393,19 @@ static cudaError_t gemm_launch_impl(bool nota, bool notb, int m, int n, int k, u
                                     void *workspace, cudaStream_t stream, const int *stop)
 {
     GemmPlan p = gemm_plan(m, n, k);
-    uint2 *Ad = reinterpret_cast<uint2 *>(workspace);
-    uint2 *Td = reinterpret_cast<uint2 *>(reinterpret_cast<unsigned char *>(workspace) + p.a_bytes);
+    double *Ad = reinterpret_cast<double *>(workspace);
+    double *Td = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(workspace) + p.a_bytes);
     unsigned char *row_nar = reinterpret_cast<unsigned char *>(workspace) + p.a_bytes + p.b_bytes;
     unsigned char *col_nar = row_nar + (size_t)p.mt * BM;
     const bool dot = !nota; // TN / TT use the dot-then-combine order
-    size_t na = p.a_bytes / sizeof(uint2), nb = p.b_bytes / sizeof(uint2);
+    size_t na = p.a_bytes / sizeof(double), nb = p.b_bytes / sizeof(double);
     cudaError_t e = cudaMemsetAsync(row_nar, 0, p.flag_bytes, stream);
     if (e != cudaSuccess)
         return e;
     decode_a_kernel<<<grid_for(na, 256), 256, 0, stream>>>(nota, m, k, A, (size_t)lda, p.kt, na, Ad, row_nar);
     decode_b_kernel<<<grid_for(nb, 256), 256, 0, stream>>>(notb, k, n, B, (size_t)ldb, !dot, alpha, p.kt, nb,
                                                            Td, col_nar);
-    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(uint2) + (size_t)RT_N * sizeof(RegimeEntry);
+    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(double) + (size_t)F64_BINADES * sizeof(uint64_t);
     dim3 grid(p.mt, p.nt);
     e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem)

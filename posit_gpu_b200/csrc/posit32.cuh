@@ -578,4 +578,123 @@ PG_HD dp32 dmac_chain(const dp32 &c, const dp32 &t, const dp32 &a)
     return r;
 }
 
+// ----------------------------------------------------------------------------
+// FP64 form
+// ----------------------------------------------------------------------------
+// A posit32 value is exact in FP64 (at most 28 significant bits, scale within +-120), so
+// p32_mul and p32_add can run on FP64 values: an FP64 operation, then rounding to the
+// posit's fraction width at the result's binade -- round to nearest even at the posit's
+// last fraction bit, done by adding and subtracting C = 1.5 * 2^(e + 52 - fb) (e the
+// binade, fb = 28 - regime run the fraction width).  The even pattern of posit rounding is
+// the even fraction, so this is the posit rounding wherever fb >= 1 (the fast window).
+PG_HD uint64_t f64_bits(double x)
+{
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+}
+PG_HD double f64_from_bits(uint64_t b)
+{
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+}
+PG_HD double f64_add(double a, double b)
+{
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(a, b); // never contracted or reassociated
+#else
+    return a + b;
+#endif
+}
+
+// C = 1.5 * 2^(e + 52 - fb) for the binade (biased FP64 exponent field) `eb`, as the
+// high word of a double whose low word is 0.
+PG_HD uint32_t f64_round_const_hi(int32_t eb)
+{
+    const int32_t k = (eb - 1023) >> 2;     // regime value
+    const int32_t run = (k ^ (k >> 31)) + 1; // regime run; fb = 28 - run
+    return ((uint32_t)(eb + 24 + run) << 20) | 0x00080000u;
+}
+
+PG_HD double f64_fma(double a, double b, double c)
+{
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return __builtin_fma(a, b, c);
+#endif
+}
+PG_HD double f64_mul(double a, double b)
+{
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+
+PG_HD bool f64_outside_fast(int32_t eb)
+{
+    return (uint32_t)(eb - 1023 - FAST_LO) > (uint32_t)(FAST_HI - FAST_LO);
+}
+
+// Biased FP64 exponent field (the binade) of x.
+PG_HD int32_t f64_binade(double x) { return (int32_t)((f64_bits(x) >> 52) & 0x7FF); }
+
+// The rounding constant for binade `eb` as FP64 bits: C = 1.5 * 2^(e + 52 - fb).  Bit 0
+// (the last mantissa bit) marks a binade outside the fast window -- there the step is
+// redone exactly and its FP64 result is discarded, so the odd constant does no harm.
+// Binade 0 holds zero (a zero product or an exactly cancelling sum): in the window.
+PG_HD uint64_t f64_round_const(int32_t eb)
+{
+    const uint64_t c = (uint64_t)f64_round_const_hi(eb) << 32;
+    return (eb != 0 && f64_outside_fast(eb)) ? (c | 1u) : c;
+}
+constexpr int F64_BINADES = 2048; // FP64 exponent fields
+struct F64ConstTable {
+    const uint64_t *tab; // f64_round_const for every binade 0..2047
+    PG_HD_MEMBER uint64_t operator()(int32_t eb) const { return tab[eb]; }
+};
+struct F64ConstComputed {
+    PG_HD_MEMBER uint64_t operator()(int32_t eb) const { return f64_round_const(eb); }
+};
+
+// c + t*a with both roundings (p32_mul, kernel_entry.cl:399-538, then p32_add,
+// kernel_entry.cl:370-397), all three posit32 values held in FP64:
+//   q = fma(t, a, Cp) - Cp    the exact product rounded once to the posit grid of its
+//                             binade (taken from fl(t*a); where that rounds up to a power
+//                             of two both give that power);
+//   r = (s + Cs) - Cs, s = c + q  the sum, exact in FP64 when the binades of c and q are at
+//                             most 24 apart; more than 30 apart the larger operand is the
+//                             result either way.
+// Bit 30 of `bad` is set when the step must be done exactly instead: a product or sum
+// binade outside the fast window, or c and q 25..30 binades apart (tested on the
+// product's binade, which is q's or one below, over the widened range 24..31).
+template <class ConstOf>
+PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, uint32_t &bad)
+{
+    const double p = f64_mul(t, a);
+    const int32_t ep = f64_binade(p);
+    const uint64_t cp = const_of(ep);
+    const double Cp = f64_from_bits(cp);
+    const double q = f64_add(f64_fma(t, a, Cp), -Cp);
+    const double s = f64_add(c, q);
+    const uint64_t cs = const_of(f64_binade(s));
+    const double Cs = f64_from_bits(cs);
+    const double r = f64_add(f64_add(s, Cs), -Cs);
+    const int32_t gap = f64_binade(c) - ep;
+    const uint32_t band = (uint32_t)((gap < 0 ? -gap : gap) - 24); // risky when <= 7
+    const bool fail = (((uint32_t)(cp | cs) & 1u) != 0) | (band <= 7u);
+    bad |= fail ? 0x40000000u : 0u;
+    return r;
+}
+
+// The same step on patterns (the exact path).  Inlined: a called function in the GEMM
+// kernels' inner loop made them fault and crawl on inputs that take this path often.
+PG_HD double f64_posit_mac_exact(double c, double t, double a)
+{
+    return p32_to_double(padd(p32_from_double(c), pmul(p32_from_double(t), p32_from_double(a))));
+}
+
 } // namespace pg

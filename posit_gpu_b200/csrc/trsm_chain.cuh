@@ -110,27 +110,6 @@ PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, in
 // than one fraction bit; this includes an exactly cancelling sum, whose FP64 value is 0).
 // The dependent path per step: three FP64 additions and a handful of integer operations
 // that build C from the exponent of s.
-PG_HD uint64_t f64_bits(double x)
-{
-    uint64_t b;
-    memcpy(&b, &x, sizeof b);
-    return b;
-}
-PG_HD double f64_from_bits(uint64_t b)
-{
-    double x;
-    memcpy(&x, &b, sizeof x);
-    return x;
-}
-PG_HD double f64_add(double a, double b)
-{
-#if defined(__CUDA_ARCH__)
-    return __dadd_rn(a, b); // never contracted or reassociated
-#else
-    return a + b;
-#endif
-}
-
 // t + q rounded to posit32, both posit values held in FP64; bit 30 of `bad` is set when
 // the step must come from the exact path instead.
 PG_HD double f64_posit_add(double t, double q, uint32_t &bad)
@@ -152,7 +131,7 @@ PG_HD double f64_posit_add(double t, double q, uint32_t &bad)
 }
 
 // The exact step on patterns (rare).
-PG_HD_NOINLINE double f64_posit_add_exact(double t, double q)
+PG_HD double f64_posit_add_exact(double t, double q)
 {
     return p32_to_double(padd(p32_from_double(t), p32_from_double(q)));
 }

@@ -120,4 +120,55 @@ long hc_f64_add_n(const uint32_t *t, const uint32_t *q, uint32_t *o, long n)
     }
     return flagged;
 }
+// c + t*a through the FP64 step (with its exact fallback) on n triples, the rounding
+// constants from a table (use_table) or computed; returns the number of steps handed to
+// the exact path.  NaR operands are handled outside (flags) by the GEMM.
+static uint64_t g_ctab[2048];
+long hc_f64_mac_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, uint32_t *o, long n, int use_table)
+{
+    for (int e = 0; e < 2048; e++)
+        g_ctab[e] = f64_round_const(e);
+    long flagged = 0;
+    for (long i = 0; i < n; i++) {
+        if (c[i] == P32_NAR || t[i] == P32_NAR || a[i] == P32_NAR) {
+            o[i] = padd(c[i], pmul(t[i], a[i]));
+            continue;
+        }
+        const double dc = p32_to_double(c[i]), dt = p32_to_double(t[i]), da = p32_to_double(a[i]);
+        uint32_t bad = 0;
+        const double r = use_table ? f64_posit_mac(dc, dt, da, F64ConstTable{g_ctab}, bad)
+                                   : f64_posit_mac(dc, dt, da, F64ConstComputed{}, bad);
+        flagged += (bad & 0x40000000u) != 0;
+        o[i] = p32_from_double((bad & 0x40000000u) ? f64_posit_mac_exact(dc, dt, da) : r);
+    }
+    return flagged;
+}
+// Pairs (t, a) whose FP64 product lies exactly on a posit rounding tie while being inexact
+// -- the one product case the FP64 step must hand to the exact path.  Random search.
+long hc_find_tie_products(uint64_t seed, long tries, uint32_t *t_out, uint32_t *a_out, long max_out)
+{
+    uint64_t x = seed | 1;
+    long found = 0;
+    for (long i = 0; i < tries && found < max_out; i++) {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        const uint32_t ut = (uint32_t)(0x40000000u | ((x >> 8) & 0x07FFFFFFu)); // [1, 2): 27 fraction bits
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        const uint32_t ua = (uint32_t)(0x40000000u | ((x >> 8) & 0x07FFFFFFu));
+        const double dt = p32_to_double(ut), da = p32_to_double(ua);
+        const double p = dt * da, e = __builtin_fma(dt, da, -p);
+        if (e == 0.0)
+            continue;
+        const int32_t ep = (int32_t)((f64_bits(p) >> 52) & 0x7FF);
+        const uint32_t hp = f64_round_const_hi(ep);
+        const double C = f64_from_bits((uint64_t)hp << 32);
+        const double q = (p + C) - C;
+        const double hulp = f64_from_bits((uint64_t)((hp & 0xFFF00000u) - (53u << 20)) << 32);
+        if (p - q == hulp || p - q == -hulp) {
+            t_out[found] = ut;
+            a_out[found] = ua;
+            found++;
+        }
+    }
+    return found;
+}
 }

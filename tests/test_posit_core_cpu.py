@@ -35,6 +35,10 @@ def hc(tmp_path_factory):
     lib.hc_chain_add.restype = ctypes.c_uint32
     lib.hc_f64_add_n.argtypes = [U32, U32, U32, ctypes.c_long]
     lib.hc_f64_add_n.restype = ctypes.c_long
+    lib.hc_f64_mac_n.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_int]
+    lib.hc_f64_mac_n.restype = ctypes.c_long
+    lib.hc_find_tie_products.argtypes = [ctypes.c_uint64, ctypes.c_long, U32, U32, ctypes.c_long]
+    lib.hc_find_tie_products.restype = ctypes.c_long
     lib.hc_decode_bf_mismatch.argtypes = [U32, ctypes.c_long]
     lib.hc_decode_bf_mismatch.restype = ctypes.c_long
     return lib
@@ -204,4 +208,53 @@ def test_fp64_chain_step_matches_oracle_across_binade_gaps(hc):
     oracle.orc.orc_p32_add_n(t, q, want, n)
     assert np.array_equal(out, want)
     assert 0 < flagged < n // 2  # near-ties sit in the risky 25..30-binade band by design
+
+
+def _oracle_mac(c, t, a):
+    p = np.empty_like(c)
+    oracle.orc.orc_p32_mul_n(t, a, p, c.size)
+    out = np.empty_like(c)
+    oracle.orc.orc_p32_add_n(c, p, out, c.size)
+    return out
+
+
+@pytest.mark.parametrize("use_table", [1, 0])
+def test_fp64_multiply_add_matches_oracle(hc, use_table):
+    """The FP64 form of c + t*a (the GEMM inner step: the product rounded once by an FMA
+    onto the posit grid, the sum rounded by a magic constant) equals
+    p32_add(c, p32_mul(t, a)) on random, wide-range, long-regime, special and cancelling
+    operands, on binade gaps across the risky band, and on products whose FP64 rounding
+    lands exactly on a posit tie."""
+    rng = np.random.default_rng(31)
+    c, t, a = _mix(rng, 60_000), _mix(rng, 60_000), _mix(rng, 60_000)
+    a[::9] = oracle.P32_ONE
+    c[::9] = (0 - t[::9].astype(np.uint64)).astype(np.uint32)  # c + t*1 == 0
+    out = np.empty_like(c)
+    hc.hc_f64_mac_n(c, t, a, out, c.size, use_table)
+    assert np.array_equal(out, _oracle_mac(c, t, a))
+    # binade gaps 0..40 between the accumulator and the product
+    n = 200_000
+    base, gap = rng.uniform(-30, 30, n), rng.integers(0, 41, n)
+    c = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 2.0 ** base * rng.uniform(1, 2, n))
+    t = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 2.0 ** (base - gap) * rng.uniform(1, 2, n))
+    a = oracle.from_double(rng.uniform(1, 2, n) * np.sign(rng.uniform(-1, 1, n)))
+    out = np.empty_like(c)
+    hc.hc_f64_mac_n(c, t, a, out, n, use_table)
+    assert np.array_equal(out, _oracle_mac(c, t, a))
+    # U[-1,1] data, the GEMM's usual diet: almost never leaves the FP64 path
+    c, t, a = (oracle.from_double(rng.uniform(-1, 1, 200_000)) for _ in range(3))
+    out = np.empty_like(c)
+    flagged = hc.hc_f64_mac_n(c, t, a, out, c.size, use_table)
+    assert np.array_equal(out, _oracle_mac(c, t, a))
+    assert flagged < c.size // 1000
+    # products whose FP64 rounding sits exactly on a posit tie (the exact product does not)
+    tt, aa = np.zeros(64, np.uint32), np.zeros(64, np.uint32)
+    found = hc.hc_find_tie_products(12345, 400_000_000, tt, aa, 64)
+    assert found >= 4
+    tt, aa = tt[:found], aa[:found]
+    for cval in (0.0, 1e-9, -3.0, 1e9):
+        cc = oracle.from_double(np.full(found, cval))
+        out = np.empty_like(cc)
+        hc.hc_f64_mac_n(cc, tt, aa, out, found, use_table)
+        assert np.array_equal(out, _oracle_mac(cc, tt, aa))
 
