@@ -171,4 +171,28 @@ long hc_find_tie_products(uint64_t seed, long tries, uint32_t *t_out, uint32_t *
     }
     return found;
 }
+// chains c <- c + t_l*a_l through the GEMM kernels' FP64 step (per-binade constants from
+// the table, exact fixups), as the kernels run them; returns the number of fixups
+long hc_f64_gemm_chains(const uint32_t *c0, const uint32_t *t, const uint32_t *a, uint32_t *o, long nchains, long len)
+{
+    for (int e = 0; e < 2048; e++)
+        g_ctab[e] = f64_round_const(e);
+    long fixes = 0;
+    for (long j = 0; j < nchains; j++) {
+        double c = p32_to_double(c0[j]);
+        for (long l = 0; l < len; l++) {
+            const double dt = p32_to_double(t[j * len + l]), da = p32_to_double(a[j * len + l]);
+            uint32_t bad = 0;
+            const double r = f64_posit_mac(c, dt, da, F64ConstTable{g_ctab}, bad);
+            if (bad) {
+                c = f64_posit_mac_exact(c, dt, da);
+                fixes++;
+            } else {
+                c = r;
+            }
+        }
+        o[j] = p32_from_double(c);
+    }
+    return fixes;
+}
 }

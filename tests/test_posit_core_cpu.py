@@ -39,6 +39,8 @@ def hc(tmp_path_factory):
     lib.hc_f64_mac_n.restype = ctypes.c_long
     lib.hc_find_tie_products.argtypes = [ctypes.c_uint64, ctypes.c_long, U32, U32, ctypes.c_long]
     lib.hc_find_tie_products.restype = ctypes.c_long
+    lib.hc_f64_gemm_chains.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_long]
+    lib.hc_f64_gemm_chains.restype = ctypes.c_long
     lib.hc_decode_bf_mismatch.argtypes = [U32, ctypes.c_long]
     lib.hc_decode_bf_mismatch.restype = ctypes.c_long
     return lib
@@ -257,4 +259,38 @@ def test_fp64_multiply_add_matches_oracle(hc, use_table):
         out = np.empty_like(cc)
         hc.hc_f64_mac_n(cc, tt, aa, out, found, use_table)
         assert np.array_equal(out, _oracle_mac(cc, tt, aa))
+
+
+@pytest.mark.parametrize("kind", ["uniform", "wide", "cancel", "mixed"])
+def test_fp64_gemm_chains_match_oracle(hc, kind):
+    """Whole GEMM k-chains through the kernels' FP64 step (per-binade constants, exact
+    fixups) equal the reference's p32_mul/p32_add order."""
+    rng = np.random.default_rng({"uniform": 41, "wide": 42, "cancel": 43, "mixed": 44}[kind])
+    nch, ln = 300, 400
+    if kind == "uniform":
+        c0 = oracle.from_double(rng.uniform(-1, 1, nch))
+        t = oracle.from_double(rng.uniform(-1, 1, nch * ln))
+        a = oracle.from_double(rng.uniform(-1, 1, nch * ln))
+    elif kind == "wide":
+        c0 = oracle.from_double(np.sign(rng.uniform(-1, 1, nch)) * 10.0 ** rng.uniform(-20, 20, nch))
+        t = oracle.from_double(np.sign(rng.uniform(-1, 1, nch * ln)) * 10.0 ** rng.uniform(-20, 20, nch * ln))
+        a = oracle.from_double(np.sign(rng.uniform(-1, 1, nch * ln)) * 10.0 ** rng.uniform(-20, 20, nch * ln))
+    elif kind == "cancel":
+        c0 = oracle.from_double(rng.choice([1.0, -1.0, 0.5], nch))
+        t = oracle.from_double(rng.choice([1.0, -1.0, 0.5, -0.5, 2.0 ** -26, -(2.0 ** -27), 0.0], nch * ln))
+        a = oracle.from_double(rng.choice([1.0, -1.0, 3.0, 2.0 ** -3], nch * ln))
+    else:
+        c0, t, a = _mix(rng, nch // 5)[:nch], _mix(rng, nch * ln // 5), _mix(rng, nch * ln // 5)
+        t, a = t[t != oracle.P32_NAR], a[a != oracle.P32_NAR]
+        t, a = np.resize(t, nch * ln), np.resize(a, nch * ln)
+        c0 = np.resize(c0[c0 != oracle.P32_NAR], nch)
+    c0, t, a = (np.ascontiguousarray(x, dtype=np.uint32) for x in (c0, t, a))
+    out = np.empty(nch, np.uint32)
+    hc.hc_f64_gemm_chains(c0, t, a, out, nch, ln)
+    want = c0.copy()
+    for l in range(ln):
+        p = np.empty(nch, np.uint32)
+        oracle.orc.orc_p32_mul_n(np.ascontiguousarray(t[l::ln]), np.ascontiguousarray(a[l::ln]), p, nch)
+        oracle.orc.orc_p32_add_n(want, p, want, nch)
+    assert np.array_equal(out, want)
 
