@@ -642,14 +642,15 @@ PG_HD bool f64_outside_fast(int32_t eb)
 // Biased FP64 exponent field (the binade) of x.
 PG_HD int32_t f64_binade(double x) { return (int32_t)((f64_bits(x) >> 52) & 0x7FF); }
 
-// The rounding constant for binade `eb` as FP64 bits: C = 1.5 * 2^(e + 52 - fb).  Bit 0
-// (the last mantissa bit) marks a binade outside the fast window -- there the step is
-// redone exactly and its FP64 result is discarded, so the odd constant does no harm.
-// Binade 0 holds zero (a zero product or an exactly cancelling sum): in the window.
+// The rounding constant for binade `eb` as FP64 bits: C = 1.5 * 2^(e + 52 - fb).  A binade
+// outside the fast window gets a NaN instead, so that a product or sum falling there comes
+// out NaN and is redone exactly.  Binade 0 holds zero (a zero product or an exactly
+// cancelling sum): in the window.
 PG_HD uint64_t f64_round_const(int32_t eb)
 {
-    const uint64_t c = (uint64_t)f64_round_const_hi(eb) << 32;
-    return (eb != 0 && f64_outside_fast(eb)) ? (c | 1u) : c;
+    if (eb != 0 && f64_outside_fast(eb))
+        return 0x7FF8000000000000ull;
+    return (uint64_t)f64_round_const_hi(eb) << 32;
 }
 constexpr int F64_BINADES = 2048; // FP64 exponent fields
 struct F64ConstTable {
@@ -665,27 +666,25 @@ struct F64ConstComputed {
 //   q = fma(t, a, Cp) - Cp    the exact product rounded once to the posit grid of its
 //                             binade (taken from fl(t*a); where that rounds up to a power
 //                             of two both give that power);
-//   r = (s + Cs) - Cs, s = c + q  the sum, exact in FP64 when the binades of c and q are at
-//                             most 24 apart; more than 30 apart the larger operand is the
-//                             result either way.
-// Bit 30 of `bad` is set when the step must be done exactly instead: a product or sum
-// binade outside the fast window, or c and q 25..30 binades apart (tested on the
-// product's binade, which is q's or one below, over the widened range 24..31).
+//   s = c + q, err            the sum and its exact rounding error (TwoSum, Knuth): when
+//                             err == 0 the FP64 sum is the exact sum;
+//   r = (s + Cs) - Cs         the exact sum rounded to the posit grid of its binade.
+// Bit 30 of `bad` is set when the step must be done exactly instead: an inexact FP64 sum
+// (err != 0), or a product or sum outside the fast window (its constant is NaN, so r is).
+// Flagging every inexact sum is conservative: beyond 30 binades the rounded sum would be
+// right anyway, but that case is rare on the data the GEMM sees.
 template <class ConstOf>
 PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, uint32_t &bad)
 {
     const double p = f64_mul(t, a);
-    const int32_t ep = f64_binade(p);
-    const uint64_t cp = const_of(ep);
-    const double Cp = f64_from_bits(cp);
+    const double Cp = f64_from_bits(const_of(f64_binade(p)));
     const double q = f64_add(f64_fma(t, a, Cp), -Cp);
     const double s = f64_add(c, q);
-    const uint64_t cs = const_of(f64_binade(s));
-    const double Cs = f64_from_bits(cs);
+    const double bq = f64_add(s, -c);
+    const double err = f64_add(f64_add(c, -f64_add(s, -bq)), f64_add(q, -bq));
+    const double Cs = f64_from_bits(const_of(f64_binade(s)));
     const double r = f64_add(f64_add(s, Cs), -Cs);
-    const int32_t gap = f64_binade(c) - ep;
-    const uint32_t band = (uint32_t)((gap < 0 ? -gap : gap) - 24); // risky when <= 7
-    const bool fail = (((uint32_t)(cp | cs) & 1u) != 0) | (band <= 7u);
+    const bool fail = (err != 0.0) | (r != r);
     bad |= fail ? 0x40000000u : 0u;
     return r;
 }
