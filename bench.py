@@ -17,8 +17,9 @@ over l) is the LU trailing update's.  Metric: posit Gop/s = 2*m*n*k / time.
   from pinned host buffers: H2D of A, B, C and D2H of C inside the timed region.
 * roofline: the main kernel against the SM issue roofline (1 warp instruction per
   cycle per SM sub-partition, 4 per SM, 148 SMs, at the SM clock sampled during the run).
-  achieved = integer-pipe warp instructions per launch / main-kernel event time, with
-  the instructions per posit multiply-add measured by ncu (posit_gpu_b200/perf.py).
+  achieved = warp instructions per launch / main-kernel event time, with the instructions
+  per posit multiply-add measured by ncu (posit_gpu_b200/perf.py); the FP64 pipe's share
+  of its own peak is reported beside it.
 * cpu_baseline: the reference's own CPU Rgemm (libRpack/Rgemm.cpp, OpenMP over columns,
   compiled here into oracle/_ref) on a column slice of the same problem, rank 0, N=1.
 * --impl reference: that CPU Rgemm alone, all host threads, each step a column slice.
@@ -274,23 +275,27 @@ def ours(args):
     ops_per_step = 2.0 * n * n * n
     value = world * ops_per_step * args.steps / (ms_max / 1e3) / 1e9
 
-    # roofline of the main kernel (issue-bound integer code)
+    # roofline of the main kernel: instruction issue (FP64 pipe the busiest pipe)
     mads = float(n) * n * n
-    main_avg_s = (main_ms / max(1, main_launches)) / 1e3
+    main_avg_s = main_ms / 1e3 / max(main_launches, 1) if main_launches else 0.0
     sm_mhz = clocks.get("sm_mhz") or perf.SM_MAX_MHZ
     peak = perf.issue_peak_warp_inst_per_s(sm_mhz)
     achieved = None
-    if perf.INT_PIPE_WARP_INST_PER_MAD and main_avg_s > 0:
-        achieved = perf.INT_PIPE_WARP_INST_PER_MAD * mads / main_avg_s
-    roofline = {"bound": "int32_issue", "achieved": achieved and round(achieved / 1e12, 4),
+    if perf.WARP_INST_PER_MAD and main_avg_s > 0:
+        achieved = perf.WARP_INST_PER_MAD * mads / main_avg_s
+    fp64_frac = (perf.FP64_WARP_INST_PER_MAD * mads / main_avg_s / perf.fp64_pipe_peak_warp_inst_per_s(sm_mhz)
+                 if main_avg_s > 0 else None)
+    roofline = {"bound": "issue", "achieved": achieved and round(achieved / 1e12, 4),
                 "peak": round(peak / 1e12, 4), "unit": "T warp-inst/s",
                 "frac": achieved and round(achieved / peak, 4),
                 "traffic": perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD and perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD * mads,
-                "kernel": "gemm_main_kernel<false>" if ta in "nN" else "gemm_main_kernel<true>",
+                "kernel": "gemm_main_kernel<false,false>" if ta in "nN" else "gemm_main_kernel<true,false>",
                 "main_kernel_ms": round(main_avg_s * 1e3, 3),
-                "posit_gop_s_main_kernel": round(2 * mads / main_avg_s / 1e9, 2),
-                "int_pipe_warp_inst_per_mad": perf.INT_PIPE_WARP_INST_PER_MAD,
-                "peak_basis": f"148 SMs x 4 SMSP x 1 warp-inst/clk at {sm_mhz:.0f} MHz (sampled median)",
+                "posit_gop_s_main_kernel": round(2 * mads / main_avg_s / 1e9, 2) if main_avg_s > 0 else None,
+                "warp_inst_per_mad": perf.WARP_INST_PER_MAD,
+                "fp64_pipe_frac": fp64_frac and round(fp64_frac, 4),
+                "peak_basis": f"148 SMs x 4 SMSP x 1 warp-inst/clk at {sm_mhz:.0f} MHz (sampled median); "
+                              "MEASURED_PEAKS.json has no issue or FP64 figure",
                 "inst_source": perf.INST_SOURCE}
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
