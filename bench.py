@@ -762,6 +762,10 @@ def main():
     if args.workload == "batch":
         return batch_arm(args)
     if args.workload == "serve":
+        # The server runs dozens of streams at once; CUDA maps streams onto this many
+        # hardware queues (default 8), and kernels of streams sharing a queue serialise.
+        # Read when the context is created, so it is set before any CUDA call.
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
         return serve_arm(args)
     return ours(args)
 

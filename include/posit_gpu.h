@@ -170,7 +170,10 @@ void posit_batch_plan_destroy(posit_batch_plan *plan);
  * Rpotrf/Rpotrs -- whether served alone, in any mix, or from the cache.  When info != 0
  * the contents of X are unspecified.  Host buffers must stay valid until the request is
  * finished; page-locked buffers are copied asynchronously, pageable ones cost a host copy
- * on the serving threads.  Multiple client threads may submit and wait concurrently. */
+ * on the serving threads.  Multiple client threads may submit and wait concurrently.
+ * The lanes are CUDA streams; CUDA maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware
+ * queues (default 8, at most 32), read when the process creates its CUDA context: set it
+ * to 32 in the environment for units on different lanes to overlap fully. */
 #define POSIT_E_QUEUE_FULL (-8)      /* the server's queue holds max_queue requests */
 #define POSIT_E_CANCELLED (-9)       /* cancelled before admission, or the server shut down */
 #define POSIT_E_NOT_CACHED (-10)     /* A == NULL and no factor is cached under matrix_id */
