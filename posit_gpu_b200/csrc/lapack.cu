@@ -207,64 +207,138 @@ __global__ void laswp_kernel(uint32_t *__restrict__ A, size_t lda, int ncols, in
 // row (strided), the column in shared memory.  Loop orders and zero skips as in
 // Rtrsm.cpp:115-156 (side = L, trans = N).
 // ---------------------------------------------------------------------------
-// lower, unit or non-unit diagonal: forward substitution (Rtrsm.cpp:139-154)
+// lower, unit or non-unit diagonal: forward substitution (Rtrsm.cpp:139-154).  The column
+// is held in shared memory as FP64 (posit32 values are exact there) and every update
+// b_i - b_k*a_ik is the FP64 multiply-add step of the GEMM (posit32.cuh, f64_posit_mac),
+// its rare flagged steps redone on patterns.  NaR travels as NaN (every step that meets
+// it is flagged and redone on patterns, which give NaR).
+PG_HD double trsm_update(double c, double t, double a)
+{
+    uint32_t bad = 0;
+    const double r = f64_posit_mac(c, t, a, F64ConstComputed{}, bad);
+    return (bad & 0x40000000u) ? f64_posit_mac_exact(c, t, a) : r;
+}
+
+// The column: staged in shared memory as FP64, or (too long for that) left in place as
+// patterns and converted at every access.
+template <bool STAGED>
+struct SolveCol {
+    double *s;
+    uint32_t *g;
+    __device__ double get(int i) const { return STAGED ? s[i] : p32_to_double(g[i]); }
+    __device__ void set(int i, double v) const
+    {
+        if (STAGED)
+            s[i] = v;
+        else
+            g[i] = p32_from_double(v);
+    }
+};
+
+template <bool STAGED>
 __global__ void trsm_lln_kernel(const uint32_t *__restrict__ L, size_t ldl, uint32_t *__restrict__ B, size_t ldb,
                                 int m, bool unit, const int *__restrict__ info)
 {
-    extern __shared__ uint32_t s_b[];
+    extern __shared__ double s_x[];
     if (info && *info < 0)
         return;
     uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        s_b[i] = bcol[i];
+    const SolveCol<STAGED> x{s_x, bcol};
+    if (STAGED)
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            s_x[i] = p32_to_double(bcol[i]);
     __syncthreads();
     for (int k = 0; k < m; ++k) {
-        uint32_t bk = s_b[k];
-        if (bk != 0) {
+        double bk = x.get(k);
+        if (bk != 0.0) {
             if (!unit) {
-                bk = pdiv(bk, L[k + (size_t)k * ldl]);
+                bk = p32_to_double(pdiv(p32_from_double(bk), L[k + (size_t)k * ldl]));
                 __syncthreads();
                 if (threadIdx.x == 0)
-                    s_b[k] = bk;
+                    x.set(k, bk);
             }
-            const uint32_t nb = pneg(bk);
+            const double nb = -bk;
+            const uint32_t *lk = L + (size_t)k * ldl;
             for (int i = k + 1 + threadIdx.x; i < m; i += blockDim.x)
-                s_b[i] = padd(s_b[i], pmul(nb, L[i + (size_t)k * ldl]));
+                x.set(i, trsm_update(x.get(i), nb, p32_to_double(lk[i])));
         }
         __syncthreads();
     }
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        bcol[i] = s_b[i];
+    if (STAGED)
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            bcol[i] = p32_from_double(s_x[i]);
 }
 
-// upper, non-unit diagonal: backward substitution (Rtrsm.cpp:121-136)
+// upper, non-unit diagonal: backward substitution (Rtrsm.cpp:121-136), as above
+template <bool STAGED>
 __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint32_t *__restrict__ B, size_t ldb,
                                 int m, bool unit, const int *__restrict__ info)
 {
-    extern __shared__ uint32_t s_b[];
+    extern __shared__ double s_x[];
     if (info && *info < 0)
         return;
     uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        s_b[i] = bcol[i];
+    const SolveCol<STAGED> x{s_x, bcol};
+    if (STAGED)
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            s_x[i] = p32_to_double(bcol[i]);
     __syncthreads();
     for (int k = m - 1; k >= 0; --k) {
-        uint32_t bk = s_b[k];
-        if (bk != 0) {
+        double bk = x.get(k);
+        if (bk != 0.0) {
             if (!unit) {
-                bk = pdiv(bk, U[k + (size_t)k * ldu]);
+                bk = p32_to_double(pdiv(p32_from_double(bk), U[k + (size_t)k * ldu]));
                 __syncthreads();
                 if (threadIdx.x == 0)
-                    s_b[k] = bk;
+                    x.set(k, bk);
             }
-            const uint32_t nb = pneg(bk);
+            const double nb = -bk;
+            const uint32_t *uk = U + (size_t)k * ldu;
             for (int i = threadIdx.x; i < k; i += blockDim.x)
-                s_b[i] = padd(s_b[i], pmul(nb, U[i + (size_t)k * ldu]));
+                x.set(i, trsm_update(x.get(i), nb, p32_to_double(uk[i])));
         }
         __syncthreads();
     }
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        bcol[i] = s_b[i];
+    if (STAGED)
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            bcol[i] = p32_from_double(s_x[i]);
+}
+
+// Forward / backward solve launches: staged when the column fits in shared memory.
+static cudaError_t launch_lln(int nrhs, int threads, const uint32_t *L, size_t ldl, uint32_t *B, size_t ldb,
+                              int m, bool unit, const int *info, cudaStream_t st)
+{
+    const size_t bytes = (size_t)m * sizeof(double);
+    if (bytes <= 227 * 1024) {
+        if (bytes > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(trsm_lln_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)bytes);
+            if (e != cudaSuccess)
+                return e;
+        }
+        trsm_lln_kernel<true><<<nrhs, threads, bytes, st>>>(L, ldl, B, ldb, m, unit, info);
+    } else {
+        trsm_lln_kernel<false><<<nrhs, threads, 0, st>>>(L, ldl, B, ldb, m, unit, info);
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_lun(int nrhs, int threads, const uint32_t *U, size_t ldu, uint32_t *B, size_t ldb,
+                              int m, bool unit, const int *info, cudaStream_t st)
+{
+    const size_t bytes = (size_t)m * sizeof(double);
+    if (bytes <= 227 * 1024) {
+        if (bytes > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(trsm_lun_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)bytes);
+            if (e != cudaSuccess)
+                return e;
+        }
+        trsm_lun_kernel<true><<<nrhs, threads, bytes, st>>>(U, ldu, B, ldb, m, unit, info);
+    } else {
+        trsm_lun_kernel<false><<<nrhs, threads, 0, st>>>(U, ldu, B, ldb, m, unit, info);
+    }
+    return cudaGetLastError();
 }
 
 // Lower, transposed (Rtrsm.cpp:175-186): one block per right-hand side; the column is
@@ -296,11 +370,87 @@ __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict
 }
 
 // The same solve split over warps (one block per right-hand side, column length m with
-// 20*m bytes of shared memory): lane 0 of warp 0 runs the chain of additions for row i
-// while warps 1..3 compute the decoded terms -a_k,i-1 * b_k of row i-1 (all but its first
-// term, whose b_i the chain is still producing) into the other half of a double buffer.
-// One barrier per row.  The chain thread forms the first term of each row itself.
+// 20*m bytes of shared memory).  Warp 0 sums row i -- its first term itself, then the
+// rest in windows of 32*LLT_SCAN_E terms, each summed as one scan over the warp
+// (trsm_chain.cuh, scan form) and cut short at the first step the scan form does not
+// cover, from where one exact step and the next window go on -- while warps
+// 1..3 compute the terms -a_k,i-1 * b_k of row i-1 (all but its first, whose b_i warp 0
+// is still producing) into the other half of a double buffer.  One barrier per row.
 constexpr int LLT_PC_THREADS = 128;
+constexpr int LLT_SCAN_E = 4;
+
+// t + q[pos] + ... + q[end-1], every addition rounded as p32_add; run by a whole warp,
+// every lane returns the result.  Windows of 32*E addends, E per lane, in the scan form
+// (trsm_chain.cuh): each lane composes its addends' step maps, a warp scan gives every
+// lane its start, every lane walks its addends from the true start, and the window ends
+// at the first step the form does not cover (the running value leaves its binade, the
+// step is risky), which is done exactly before the next window starts.
+template <int E>
+__device__ double warp_chain_scan(double t, const double *q, int pos, int end)
+{
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    while (pos < end) {
+        SegParams sp;
+        if (!seg_begin(t, sp)) { // zero, or outside the fast window: one exact step
+            t = chain_add_one(t, q[pos]);
+            ++pos;
+            continue;
+        }
+        const int wend = min(end, pos + 32 * E);
+        const int j0 = pos + lane * E;
+        SegFn fe[E];
+        int32_t K[E];
+        bool rk[E];
+        SegFn f = {0, 0};
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double qv = j0 + e < wend ? q[j0 + e] : 0.0; // 0 is the identity map
+            fe[e] = seg_fn(qv, sp, K[e], rk[e]);
+            f = seg_then(f, fe[e]);
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            SegFn o;
+            o.c0 = __shfl_up_sync(FULL, f.c0, off);
+            o.c1 = __shfl_up_sync(FULL, f.c1, off);
+            if (lane >= off)
+                f = seg_then(o, f);
+        }
+        SegFn ex;
+        ex.c0 = __shfl_up_sync(FULL, f.c0, 1);
+        ex.c1 = __shfl_up_sync(FULL, f.c1, 1);
+        if (lane == 0)
+            ex = SegFn{0, 0};
+        int32_t M = seg_apply(ex, sp.M0);
+        int jbad = -1;
+        int32_t Mbad = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const bool live = (jbad < 0) & (j0 + e < wend);
+            const bool ok = seg_valid(M, K[e], rk[e], sp);
+            if (live & !ok) {
+                jbad = j0 + e;
+                Mbad = M;
+            }
+            if (live & ok)
+                M = seg_apply(fe[e], M);
+        }
+        const unsigned bal = __ballot_sync(FULL, jbad >= 0);
+        if (bal == 0) {
+            const int last = (wend - 1 - pos) / E; // the lane holding the window's last addend
+            t = sp.us * (double)__shfl_sync(FULL, M, last);
+            pos = wend;
+        } else {
+            const int src = __ffs(bal) - 1;
+            const int js = __shfl_sync(FULL, jbad, src);
+            const int32_t Ms = __shfl_sync(FULL, Mbad, src);
+            t = chain_add_one(sp.us * (double)Ms, q[js]);
+            pos = js + 1;
+        }
+    }
+    return t;
+}
 
 __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint32_t *__restrict__ L, size_t ldl,
                                                                      uint32_t *__restrict__ B, size_t ldb, int m,
@@ -319,24 +469,28 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
     if (tid < 2)
         s_nar[tid] = 0;
     __syncthreads();
+    uint32_t xprev = 0; // b_{i+1}, final (warp 0)
     for (int i = m - 1; i >= 0; --i) {
         const int cur = i & 1;
-        if (tid == 0) {
+        if (tid < 32) {
             const uint32_t *li = L + (size_t)i * ldl;
             const uint32_t bi = s_b[i];
             uint32_t nar = (bi == P32_NAR) | s_nar[cur];
             double c = p32_to_double(bi == P32_NAR ? 0u : bi);
             if (i + 1 < m) {
-                const double q0 = llt_term(li[i + 1], s_b[i + 1], &nar);
-                c = chain_add_run(c, &q0, 1);
-                c = chain_add_run(c, s_q + (size_t)cur * m + (i + 2), m - i - 2);
+                c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
+                c = warp_chain_scan<LLT_SCAN_E>(c, s_q + (size_t)cur * m, i + 2, m);
             }
             uint32_t t = nar ? P32_NAR : p32_from_double(c);
             if (!unit)
                 t = pdiv(t, li[i]);
-            s_b[i] = t;
-            s_nar[cur] = 0;
-        } else if (tid >= 32 && i >= 1) {
+            xprev = t;
+            __syncwarp();
+            if (tid == 0) {
+                s_b[i] = t;
+                s_nar[cur] = 0;
+            }
+        } else if (i >= 1) {
             // terms k = i+1 .. m-1 of row i-1 (their b_k are final)
             const uint32_t *lp = L + (size_t)(i - 1) * ldl;
             double *qn = s_q + (size_t)(cur ^ 1) * m;
@@ -485,9 +639,11 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
             uint32_t *A12 = A + j + (size_t)(j + jb) * L;
             laswp_kernel<<<(nr + 127) / 128, 128, 0, st>>>(A + (size_t)(j + jb) * L, L, nr, j + 1, j + jb, ipiv, 1,
                                                           info);
-            trsm_lln_kernel<<<nr, 256, (size_t)jb * 4, st>>>(P, L, A12, L, jb, true, info);
+            cudaError_t e = launch_lln(nr, 256, P, L, A12, L, jb, true, info, st);
+            if (e != cudaSuccess)
+                return e;
             if (j + jb < m) {
-                cudaError_t e = gemm_launch(true, true, m - j - jb, nr, jb, 0xC0000000u /* -1 */,
+                e = gemm_launch(true, true, m - j - jb, nr, jb, 0xC0000000u /* -1 */,
                                             A + (j + jb) + (size_t)j * L, lda, A12, lda, P32_ONE,
                                             A + (j + jb) + (size_t)(j + jb) * L, lda, gws, st);
                 if (e != cudaSuccess)
@@ -538,39 +694,24 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
 }
 
 // Rgetrs.cpp:84-114 (trans = 'N'): interchanges, L (unit) forward, U backward.
-static cudaError_t solve_smem(size_t bytes)
-{
-    if (bytes <= 48 * 1024)
-        return cudaSuccess;
-    if (bytes > 227 * 1024)
-        return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(trsm_lln_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(trsm_lun_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    return e;
-}
-
 cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb,
                           cudaStream_t st)
 {
     const int threads = 1024;
-    cudaError_t e = solve_smem((size_t)n * 4);
-    if (e != cudaSuccess)
-        return e;
     laswp_kernel<<<(nrhs + 127) / 128, 128, 0, st>>>(B, ldb, nrhs, 1, n, ipiv, 1, nullptr);
-    trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, true, nullptr);
-    trsm_lun_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
-    return cudaGetLastError();
+    cudaError_t e = launch_lln(nrhs, threads, A, lda, B, ldb, n, true, nullptr, st);
+    if (e == cudaSuccess)
+        e = launch_lun(nrhs, threads, A, lda, B, ldb, n, false, nullptr, st);
+    return e;
 }
 
 // Rpotrs.cpp:95-106 (uplo = 'L'): L forward, L^T backward.
 cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
 {
     const int threads = 1024;
-    cudaError_t e = solve_smem((size_t)n * 4);
+    cudaError_t e = launch_lln(nrhs, threads, A, lda, B, ldb, n, false, nullptr, st);
     if (e != cudaSuccess)
         return e;
-    trsm_lln_kernel<<<nrhs, threads, (size_t)n * 4, st>>>(A, lda, B, ldb, n, false, nullptr);
     const size_t pc = llt_pc_smem_bytes(n);
     if (pc <= (size_t)LLT_SMEM_MAX) {
         if (pc > 48 * 1024) {

@@ -3,6 +3,8 @@
 #include "../posit_gpu_b200/csrc/posit32.cuh"
 #include "../posit_gpu_b200/csrc/trsm_chain.cuh"
 #include <stdint.h>
+#include <algorithm>
+#include <vector>
 using namespace pg;
 static RegimeEntry g_table[RT_N];
 static const RegimeEntry *table()
@@ -194,5 +196,162 @@ long hc_f64_gemm_chains(const uint32_t *c0, const uint32_t *t, const uint32_t *a
         o[j] = p32_from_double(c);
     }
     return fixes;
+}
+
+// One row's chain t + q_0 + ... + q_{len-1} the way lapack.cu's warp_chain_scan runs it,
+// written out sequentially: one warp takes a window of
+// the next 32*E terms, E per lane; each lane's composed map, the exclusive prefix over
+// lanes, every lane's walk from its true start, the first invalid step of the window;
+// the window advances past it by one exact step (or past its end).
+static double scan_row_emul(double t, const double *q, int len, int E, long *segs, long *exact)
+{
+    constexpr int LANES = 32;
+    SegFn start[LANES];
+    int pos = 0;
+    while (pos < len) {
+        SegParams sp;
+        if (!seg_begin(t, sp)) {
+            t = chain_add_one(t, q[pos]);
+            ++pos;
+            ++*exact;
+            continue;
+        }
+        ++*segs;
+        const int end = std::min(len, pos + LANES * E);
+        SegFn acc = {0, 0};
+        for (int l = 0; l < LANES; ++l) {
+            start[l] = acc;
+            SegFn f = {0, 0};
+            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
+            for (int j = j0; j < j1; ++j) {
+                int32_t K;
+                bool r;
+                f = seg_then(f, seg_fn(q[j], sp, K, r));
+            }
+            acc = seg_then(acc, f);
+        }
+        uint64_t key = ~0ull;
+        int32_t Mend = 0;
+        for (int l = 0; l < LANES; ++l) {
+            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
+            int32_t M = seg_apply(start[l], sp.M0);
+            for (int j = j0; j < j1; ++j) {
+                int32_t K;
+                bool r;
+                const SegFn f = seg_fn(q[j], sp, K, r);
+                if (!seg_valid(M, K, r, sp)) {
+                    key = std::min(key, ((uint64_t)j << 32) | (uint32_t)M);
+                    break;
+                }
+                M = seg_apply(f, M);
+            }
+            if (j1 == end && j0 < end)
+                Mend = M;
+        }
+        if (key == ~0ull) {
+            t = sp.us * (double)Mend;
+            pos = end;
+        } else {
+            const int js = (int)(key >> 32);
+            t = chain_add_one(sp.us * (double)(int32_t)(uint32_t)key, q[js]);
+            pos = js + 1;
+            ++*exact;
+        }
+    }
+    return t;
+}
+
+// The two-binade scan form (Seg2*) as lapack.cu's warp_chain_scan runs it: per window,
+// the addends in units of v, the running sum of their integer parts for the side
+// predictions, the lanes' composed maps, their walks from their true starts.
+static double scan_row_emul2(double t, const double *q, int len, int E, long *segs, long *exact)
+{
+    constexpr int LANES = 32;
+    std::vector<Seg2Fn> start(LANES);
+    std::vector<double> Q(LANES * E), P(LANES * E);
+    int pos = 0;
+    while (pos < len) {
+        Seg2Params sp;
+        if (!seg2_begin(t, sp)) {
+            t = chain_add_one(t, q[pos]);
+            ++pos;
+            ++*exact;
+            continue;
+        }
+        ++*segs;
+        const int end = std::min(len, pos + LANES * E);
+        uint32_t run = (uint32_t)sp.N0; // side predictions as lapack.cu makes them
+        for (int j = pos; j < end; ++j) {
+            Q[j - pos] = q[j] * sp.w;
+            run += (uint32_t)seg2_floor(Q[j - pos]);
+            P[j - pos] = (double)(int32_t)run;
+        }
+        Seg2Fn acc = {{0, 0, 0, 0}};
+        for (int l = 0; l < LANES; ++l) {
+            start[l] = acc;
+            Seg2Fn f = {{0, 0, 0, 0}};
+            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
+            for (int j = j0; j < j1; ++j) {
+                int32_t K, lo, span;
+                f = seg2_then(f, seg2_fn(Q[j - pos], P[j - pos] >= sp.mid, sp, K, lo, span));
+            }
+            acc = seg2_then(acc, f);
+        }
+        uint64_t key = ~0ull;
+        int32_t Nend = 0;
+        for (int l = 0; l < LANES; ++l) {
+            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
+            int32_t N = seg2_apply(start[l], sp.N0);
+            for (int j = j0; j < j1; ++j) {
+                int32_t K, lo, span;
+                const Seg2Fn f = seg2_fn(Q[j - pos], P[j - pos] >= sp.mid, sp, K, lo, span);
+                if (!seg2_valid(N, K, lo, span, sp)) {
+                    key = std::min(key, ((uint64_t)j << 32) | (uint32_t)N);
+                    break;
+                }
+                N = seg2_apply(f, N);
+            }
+            if (j1 == end && j0 < end)
+                Nend = N;
+        }
+        if (key == ~0ull) {
+            t = sp.vs * (double)Nend;
+            pos = end;
+        } else {
+            const int js = (int)(key >> 32);
+            t = chain_add_one(sp.vs * (double)(int32_t)(uint32_t)key, q[js]);
+            pos = js + 1;
+            ++*exact;
+        }
+    }
+    return t;
+}
+// The L^T solve with rows summed by scan_row_emul; stats[0] += scans, stats[1] += exact steps.
+void hc_llt_solve_scan(const uint32_t *L, long ld, uint32_t *b, int m, int E, long *stats)
+{
+    std::vector<double> q(m > 0 ? m : 1);
+    for (int i = m - 1; i >= 0; --i) {
+        const uint32_t *li = L + (long)i * ld;
+        uint32_t nar = b[i] == P32_NAR;
+        const int len = m - 1 - i;
+        for (int j = 0; j < len; ++j)
+            q[j] = llt_term(li[i + 1 + j], b[i + 1 + j], &nar);
+        const double t0 = p32_to_double(b[i] == P32_NAR ? 0u : b[i]);
+        const double c = E > 0 ? scan_row_emul(t0, q.data(), len, E, &stats[0], &stats[1])
+                               : scan_row_emul2(t0, q.data(), len, -E, &stats[0], &stats[1]);
+        uint32_t t = nar ? P32_NAR : p32_from_double(c);
+        b[i] = pdiv(t, li[i]);
+    }
+}
+// scan_row_emul against chain_add_run on one chain of n terms (patterns); returns 1 on a match
+int hc_scan_row_check(uint32_t c0, const uint32_t *qp, int n, int E, long *stats)
+{
+    std::vector<double> q(n > 0 ? n : 1);
+    for (int k = 0; k < n; ++k)
+        q[k] = p32_to_double(qp[k]);
+    const double a = chain_add_run(p32_to_double(c0), q.data(), n);
+    const double b = E > 0 ? scan_row_emul(p32_to_double(c0), q.data(), n, E, &stats[0], &stats[1])
+                           : scan_row_emul2(p32_to_double(c0), q.data(), n, -E, &stats[0], &stats[1]);
+    return p32_from_double(a) == p32_from_double(b);
 }
 }

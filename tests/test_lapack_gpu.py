@@ -102,6 +102,34 @@ def test_rpotrs_bit_exact(cuda_ok, n, nrhs):
     assert np.array_equal(g, o)
 
 
+@pytest.mark.parametrize("n,kind", [(300, "wide"), (700, "ties"), (1500, "u")])
+def test_rpotrs_any_factor_bit_exact(cuda_ok, n, kind):
+    """Rpotrs on lower triangles that are no Cholesky factor: entries over 40 decades, or
+    powers of two that make the running sums hit grid ties, zeros in the right-hand sides,
+    a NaR in one column -- the transposed solve's chain leaves its binade, cancels and
+    takes the exact path often."""
+    import posit_gpu_b200 as pg
+    rng = np.random.default_rng(n)
+    if kind == "wide":
+        Lf = np.sign(rng.uniform(-1, 1, (n, n))) * 10.0 ** rng.uniform(-20, 20, (n, n))
+    elif kind == "ties":
+        Lf = rng.choice([-1, 1], (n, n)) * 2.0 ** -rng.integers(0, 30, (n, n))
+    else:
+        Lf = rng.uniform(-1, 1, (n, n)) / np.sqrt(n)
+    Lf = np.tril(Lf)
+    np.fill_diagonal(Lf, 1.0 + rng.uniform(0, 1, n))
+    L = oracle.from_double(Lf.reshape(-1, order="F"))
+    nrhs = 3
+    B = oracle.from_double(rng.uniform(-1, 1, n * nrhs))
+    B[::7] = 0
+    if kind == "wide":
+        L[(n - 1) + 5 * n] = oracle.P32_NAR  # column 5 of L^T's row: x_5 and those above it NaR
+    g, o = B.copy(), B.copy()
+    pg.Rpotrs("L", n, nrhs, L, n, g, n)
+    oracle.orc.orc_rpotrs(b"L", n, nrhs, L, n, o, n)
+    assert np.array_equal(g, o)
+
+
 def test_lapack_matches_reference_golden(cuda_ok):
     """LU, Cholesky and both solves against outputs of the reference's own code."""
     import posit_gpu_b200 as pg

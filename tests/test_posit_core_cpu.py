@@ -13,6 +13,7 @@ import oracle
 HERE = os.path.dirname(os.path.abspath(__file__))
 U32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 F64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+I64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 
 
 @pytest.fixture(scope="module")
@@ -31,6 +32,8 @@ def hc(tmp_path_factory):
     lib.hc_dmac_chain_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
     lib.hc_llt_solve.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
     lib.hc_llt_solve_split.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
+    lib.hc_llt_solve_scan.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int, ctypes.c_int, I64]
+    lib.hc_scan_row_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int, ctypes.c_int, I64]
     lib.hc_chain_add.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.restype = ctypes.c_uint32
     lib.hc_f64_add_n.argtypes = [U32, U32, U32, ctypes.c_long]
@@ -154,6 +157,10 @@ def test_lower_transposed_solve_matches_oracle(hc):
             got = b.copy()
             solve(L, m, got, m)
             assert np.array_equal(got, want), (m, kind, solve.__name__)
+        for E in (1, 4, -1, -8):  # E < 0: the two-binade form
+            got = b.copy()
+            hc.hc_llt_solve_scan(L, m, got, m, E, np.zeros(2, np.int64))
+            assert np.array_equal(got, want), (m, kind, "scan", E)
 
 
 def test_branch_free_decode_matches_decode(hc):
@@ -294,3 +301,33 @@ def test_fp64_gemm_chains_match_oracle(hc, kind):
         oracle.orc.orc_p32_add_n(want, p, want, nch)
     assert np.array_equal(out, want)
 
+
+
+def test_scan_form_of_the_chain_matches_sequential_additions(hc):
+    """The scan forms of a chain of additions (step maps M -> M + c[M & 1] on the posit grid
+    of the running value's binade, or N -> N + c[N & 3] over two adjacent binades, composed
+    over a warp's window, cut at the first step the form does not cover) equal
+    chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
+    cancel to zero, hit ties (halves of the grid spacing), span 80 decades, and carry addends
+    25..30 binades down."""
+    rng = np.random.default_rng(31)
+    stats = np.zeros(2, np.int64)
+    for trial in range(1200):
+        n = int(rng.integers(0, 1500))
+        kind = trial % 6
+        if kind == 0:
+            q = oracle.from_double(rng.uniform(-1, 1, n) * 0.01)
+        elif kind == 1:
+            q = oracle.from_double(np.sign(rng.uniform(-1, 1, n)) * 10.0 ** rng.uniform(-40, 40, n))
+        elif kind == 2:
+            q = oracle.from_double(rng.choice([-1.0, 1.0, 0.5, -0.5, 0.0, 3.0, -3.0, 2**-20, -2**-27], n))
+        elif kind == 3:
+            q = oracle.from_double(rng.uniform(-1, 1, n) * 2.0 ** rng.integers(-30, 2, n))
+        elif kind == 4:  # halves and quarters of the spacing near 1: ties on both parities
+            q = oracle.from_double(rng.choice([-1, 1], n) * 2.0 ** -rng.integers(26, 30, n))
+        else:  # addends 24..31 binades below a running value near 1
+            q = oracle.from_double(rng.choice([-1, 1], n) * 2.0 ** -rng.integers(24, 32, n) * rng.uniform(1, 2, n))
+        c0 = int(oracle.from_double(np.array([rng.uniform(-2, 2)]))[0])
+        E = int(rng.choice([1, 2, 4, 8, -1, -2, -4, -8]))  # E < 0: the two-binade form
+        assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
+    assert stats[0] > 0 and stats[1] > 0  # both scans and exact steps were exercised
