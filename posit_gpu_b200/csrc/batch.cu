@@ -18,6 +18,41 @@ namespace {
 
 constexpr int BT = 256; // threads per problem
 
+// The per-element steps are the FP64 form of p32_mul + p32_add (posit32.cuh,
+// f64_posit_mac_checked): operands converted from patterns, the result assembled back
+// without rounding.  Row k and column k of a factor step are staged in shared memory as
+// FP64 when 2n doubles fit in the staging buffer.
+constexpr int STAGE_DOUBLES = BATCH_MAX_N / 2; // s_row (BATCH_MAX_N words) as FP64
+
+__device__ __forceinline__ double pd(uint32_t u) { return p32_to_double(u); }
+
+// b <- b + t*a on patterns through the FP64 step
+__device__ __forceinline__ void mac_store(uint32_t *p, double t, double a)
+{
+    *p = p32_from_double_exact(f64_posit_mac_checked(pd(*p), t, a));
+}
+
+// Walks the rows x rows trailing block of step k as flat indexes e = tid, tid + BT, ...
+// (row fastest) without a division per element.
+struct TrailWalk {
+    int i, c;           // the current element (row, column)
+    int di, dc, lo, hi; // the step, and the row range [lo, hi)
+    __device__ TrailWalk(int rows, int k)
+        : i(k + 1 + (int)threadIdx.x % rows), c(k + 1 + (int)threadIdx.x / rows), di(BT % rows), dc(BT / rows),
+          lo(k + 1), hi(k + 1 + rows)
+    {
+    }
+    __device__ void next()
+    {
+        i += di;
+        c += dc;
+        if (i >= hi) {
+            i -= hi - lo;
+            ++c;
+        }
+    }
+};
+
 __device__ int iramax_block(const uint32_t *col, int k, int n, int32_t *s_key, int *s_idx)
 {
     const int tid = threadIdx.x;
@@ -95,15 +130,27 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
                 l = pdiv(l, s_piv);
             ck[i] = l;
         }
-        for (int c = k + 1 + tid; c < n; c += blockDim.x)
-            s_row[c] = pneg(A[k + (size_t)c * lda]);
+        const bool stage = 2 * n <= STAGE_DOUBLES;
+        double *s_rowd = reinterpret_cast<double *>(s_row), *s_cold = s_rowd + n;
+        for (int c = k + 1 + tid; c < n; c += blockDim.x) {
+            const uint32_t v = pneg(A[k + (size_t)c * lda]);
+            if (stage)
+                s_rowd[c] = pd(v);
+            else
+                s_row[c] = v;
+        }
+        if (stage)
+            for (int i = k + 1 + tid; i < n; i += blockDim.x)
+                s_cold[i] = pd(ck[i]);
         __syncthreads();
         const int rows = n - k - 1;
-        const int cnt = rows * rows;
-        for (int e = tid; e < cnt; e += blockDim.x) {
-            const int i = k + 1 + e % rows, c = k + 1 + e / rows;
-            uint32_t *pc = A + i + (size_t)c * lda;
-            *pc = padd(*pc, pmul(s_row[c], ck[i]));
+        if (rows > 0) {
+            TrailWalk w(rows, k);
+            for (; w.c < n; w.next()) {
+                const double t = stage ? s_rowd[w.c] : pd(s_row[w.c]);
+                const double l = stage ? s_cold[w.i] : pd(ck[w.i]);
+                mac_store(A + w.i + (size_t)w.c * lda, t, l);
+            }
         }
         __syncthreads();
     }
@@ -133,7 +180,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
             const int i = k + 1 + e % rows;
             const uint32_t bk = b[k];
             if (bk != 0)
-                b[i] = padd(b[i], pmul(pneg(bk), lk[i]));
+                mac_store(b + i, -pd(bk), pd(lk[i]));
         }
         __syncthreads();
     }
@@ -150,7 +197,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
             const int i = e % k;
             const uint32_t bk = b[k];
             if (bk != 0)
-                b[i] = padd(b[i], pmul(pneg(bk), uk[i]));
+                mac_store(b + i, -pd(bk), pd(uk[i]));
         }
         __syncthreads();
     }
@@ -181,20 +228,27 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
             info = k + 1;
             break;
         }
+        const bool stage = n <= STAGE_DOUBLES;
+        double *s_cold = reinterpret_cast<double *>(s_row);
         for (int i = k + 1 + tid; i < n; i += blockDim.x) {
             const uint32_t l = pmul(s_recip, ck[i]);
             ck[i] = l;
-            s_row[i] = pneg(l);
+            if (stage)
+                s_cold[i] = pd(l);
+            else
+                s_row[i] = l;
         }
         __syncthreads();
         // lower part of the trailing matrix: a_ic += (-l_ck)*l_ik, k < c <= i
         const int rows = n - k - 1;
-        const int cnt = rows * rows;
-        for (int e = tid; e < cnt; e += blockDim.x) {
-            const int i = k + 1 + e % rows, c = k + 1 + e / rows;
-            if (i >= c) {
-                uint32_t *pc = A + i + (size_t)c * lda;
-                *pc = padd(*pc, pmul(s_row[c], ck[i]));
+        if (rows > 0) {
+            TrailWalk w(rows, k);
+            for (; w.c < n; w.next()) {
+                if (w.i >= w.c) {
+                    const double lc = stage ? s_cold[w.c] : pd(s_row[w.c]);
+                    const double li = stage ? s_cold[w.i] : pd(s_row[w.i]);
+                    mac_store(A + w.i + (size_t)w.c * lda, -lc, li);
+                }
             }
         }
         __syncthreads();
@@ -221,7 +275,7 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
             const int i = k + 1 + e % rows;
             const uint32_t bk = b[k];
             if (bk != 0)
-                b[i] = padd(b[i], pmul(pneg(bk), lk[i]));
+                mac_store(b + i, -pd(bk), pd(lk[i]));
         }
         __syncthreads();
     }
@@ -241,13 +295,16 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
 
 } // namespace
 
-__global__ void __launch_bounds__(BT) batch_factor_kernel(const BatchProblem *__restrict__ probs, int nprob,
+#ifndef PG_BATCH_MIN_CTAS
+#define PG_BATCH_MIN_CTAS 4 // 64 registers: 4 resident CTAs per SM (measured best of 2, 3, 4)
+#endif
+__global__ void __launch_bounds__(BT, PG_BATCH_MIN_CTAS) batch_factor_kernel(const BatchProblem *__restrict__ probs, int nprob,
                                                           const int *__restrict__ order, int *__restrict__ next)
 {
     __shared__ int32_t s_key[BT];
     __shared__ int s_idx[BT];
     __shared__ int s_item;
-    __shared__ uint32_t s_row[BATCH_MAX_N];
+    __shared__ __align__(16) uint32_t s_row[BATCH_MAX_N]; // also staged FP64 (8-byte aligned)
     for (;;) {
         if (threadIdx.x == 0)
             s_item = atomicAdd(next, 1);

@@ -378,13 +378,16 @@ __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict
 // is still producing) into the other half of a double buffer.  One barrier per row.
 constexpr int LLT_PC_THREADS = 128;
 constexpr int LLT_SCAN_E = 4;
+constexpr int LLT_SHORT_WINDOW = 64; // a window that ends sooner ...
+constexpr int LLT_SEQ_STEPS = 32;    // ... is followed by this many sequential steps
 
 // t + q[pos] + ... + q[end-1], every addition rounded as p32_add; run by a whole warp,
 // every lane returns the result.  Windows of 32*E addends, E per lane, in the scan form
 // (trsm_chain.cuh): each lane composes its addends' step maps, a warp scan gives every
 // lane its start, every lane walks its addends from the true start, and the window ends
 // at the first step the form does not cover (the running value leaves its binade, the
-// step is risky), which is done exactly before the next window starts.
+// step is risky), which is done exactly before the next window starts.  Where windows
+// keep ending early, short runs of sequential steps (chain_add_run_reg) go in between.
 template <int E>
 __device__ double warp_chain_scan(double t, const double *q, int pos, int end)
 {
@@ -446,7 +449,15 @@ __device__ double warp_chain_scan(double t, const double *q, int pos, int end)
             const int js = __shfl_sync(FULL, jbad, src);
             const int32_t Ms = __shfl_sync(FULL, Mbad, src);
             t = chain_add_one(sp.us * (double)Ms, q[js]);
+            // A window cut short means a running value that keeps changing binade (it is
+            // small against its addends): the next LLT_SEQ_STEPS steps go one by one.
+            const bool cut_short = js - pos < LLT_SHORT_WINDOW;
             pos = js + 1;
+            if (cut_short) {
+                const int cnt = min(LLT_SEQ_STEPS, end - pos);
+                t = chain_add_run_reg(t, q + pos, cnt);
+                pos += cnt;
+            }
         }
     }
     return t;

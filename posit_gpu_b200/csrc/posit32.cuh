@@ -697,4 +697,31 @@ PG_HD double f64_posit_mac_exact(double c, double t, double a)
     return p32_to_double(padd(p32_from_double(c), pmul(p32_from_double(t), p32_from_double(a))));
 }
 
+// c + t*a with the exact path taken where the FP64 step is flagged.
+PG_HD double f64_posit_mac_checked(double c, double t, double a)
+{
+    uint32_t bad = 0;
+    const double r = f64_posit_mac(c, t, a, F64ConstComputed{}, bad);
+    return (bad & 0x40000000u) ? f64_posit_mac_exact(c, t, a) : r;
+}
+
+// FP64 -> posit32 for a value that IS a posit32 value (an output of the FP64 steps or of
+// p32_to_double): the fields are assembled without rounding.  Regimes longer than 27 bits
+// (fewer than one fraction bit) and NaN go through p32_from_double.
+PG_HD uint32_t p32_from_double_exact(double x)
+{
+    const uint64_t b = f64_bits(x);
+    const int32_t s = (int32_t)((b >> 52) & 0x7FF) - 1023;
+    if ((b << 1) == 0)
+        return 0;
+    if ((uint32_t)(s - FAST_LO) > (uint32_t)(FAST_HI - FAST_LO))
+        return p32_from_double(x);
+    const int32_t k = s >> 2;
+    const uint32_t run = (uint32_t)((k ^ (k >> 31)) + 1); // regime run; fraction bits 28 - run
+    const uint32_t reg = k >= 0 ? ((1u << run) - 1u) << 1 : 1u; // the run+1 regime bits
+    const uint32_t u = (reg << (30 - run)) | ((uint32_t)(s & 3) << (28 - run)) |
+                       (uint32_t)((b & 0xFFFFFFFFFFFFFull) >> (24 + run));
+    return (b >> 63) ? 0u - u : u;
+}
+
 } // namespace pg

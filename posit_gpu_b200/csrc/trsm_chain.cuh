@@ -297,6 +297,70 @@ PG_HD double chain_add_one(double t, double q)
 }
 
 
+
+// ---------------------------------------------------------------------------
+// The chain step with the regime held fixed.
+// ---------------------------------------------------------------------------
+// In f64_posit_add the rounding constant is built from the sum's exponent with integer
+// operations on the dependent path.  Within one regime (4 binades) the fraction width is
+// fixed, so C = 2^e * G with G = 1.5 * 2^(52 - fb) the regime's gain, and 2^e is the sum
+// with its sign and fraction bits masked off: one AND and one FP64 multiply.  The regime
+// is taken from the value a block of steps starts at; a step whose sum lands in another
+// regime (or is zero, or is risky as in f64_posit_add) is flagged, and the caller redoes
+// the block with chain_add_one.
+PG_HD double f64_regime_gain(int32_t k)
+{
+    const int32_t fb = 28 - ((k ^ (k >> 31)) + 1);
+    return f64_from_bits(((uint64_t)(uint32_t)(52 - fb + 1023) << 52) | 0x0008000000000000ull);
+}
+
+PG_HD int32_t f64_regime(double x) { return ((int32_t)((f64_bits(x) >> 52) & 0x7FF) - 1023) >> 2; }
+
+PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint32_t &bad)
+{
+    const double s = f64_add(t, q);
+    const uint64_t sb = f64_bits(s);
+    const double C = f64_mul(f64_from_bits(sb & 0x7FF0000000000000ull), G);
+    const double r = f64_add(f64_add(s, C), -C);
+    // off the dependent path
+    const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
+    const int32_t gap = et > eq ? et - eq : eq - et;
+    const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
+    const int32_t ks = ((int32_t)((sb >> 52) & 0x7FF) - 1023) >> 2;
+    bad |= (risky | (ks != kreg)) ? 0x40000000u : 0u;
+    return r;
+}
+
+// t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-regime step: blocks of
+// CHAIN_BLOCK steps without a branch, a flagged block redone step by step exactly.
+PG_HD double chain_add_run_reg(double t, const double *q, int count)
+{
+    constexpr int U = CHAIN_BLOCK;
+    int k = 0;
+    for (; k + U <= count; k += U) {
+        const int32_t kreg = f64_regime(t);
+        const bool in = (t != 0.0) & (kreg >= (FAST_LO >> 2)) & (kreg <= (FAST_HI >> 2));
+        const double G = f64_regime_gain(kreg);
+        double v[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            v[j] = q[k + j];
+        const double t0 = t;
+        uint32_t bad = in ? 0u : 0x40000000u;
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            t = f64_posit_add_reg(t, v[j], G, kreg, bad);
+        if (bad & 0x40000000u) {
+            t = t0;
+            for (int j = 0; j < U; ++j)
+                t = chain_add_one(t, v[j]);
+        }
+    }
+    for (; k < count; ++k)
+        t = chain_add_one(t, q[k]);
+    return t;
+}
+
 // ---------------------------------------------------------------------------
 // Scan form over two adjacent binades.
 // ---------------------------------------------------------------------------

@@ -202,7 +202,8 @@ long hc_f64_gemm_chains(const uint32_t *c0, const uint32_t *t, const uint32_t *a
 // written out sequentially: one warp takes a window of
 // the next 32*E terms, E per lane; each lane's composed map, the exclusive prefix over
 // lanes, every lane's walk from its true start, the first invalid step of the window;
-// the window advances past it by one exact step (or past its end).
+// the window advances past it by one exact step (or past its end); a window that ended
+// within 64 addends is followed by 32 sequential steps.
 static double scan_row_emul(double t, const double *q, int len, int E, long *segs, long *exact)
 {
     constexpr int LANES = 32;
@@ -254,8 +255,14 @@ static double scan_row_emul(double t, const double *q, int len, int E, long *seg
         } else {
             const int js = (int)(key >> 32);
             t = chain_add_one(sp.us * (double)(int32_t)(uint32_t)key, q[js]);
+            const bool cut_short = js - pos < 64; // lapack.cu: LLT_SHORT_WINDOW, LLT_SEQ_STEPS
             pos = js + 1;
             ++*exact;
+            if (cut_short) {
+                const int cnt = std::min(32, len - pos);
+                t = chain_add_run_reg(t, q + pos, cnt);
+                pos += cnt;
+            }
         }
     }
     return t;
@@ -342,6 +349,24 @@ void hc_llt_solve_scan(const uint32_t *L, long ld, uint32_t *b, int m, int E, lo
         uint32_t t = nar ? P32_NAR : p32_from_double(c);
         b[i] = pdiv(t, li[i]);
     }
+}
+// p32_from_double_exact(p32_to_double(u)) == u over n patterns; returns mismatches
+long hc_from_double_exact_mismatch(const uint32_t *u, long n)
+{
+    long bad = 0;
+    for (long i = 0; i < n; i++)
+        bad += p32_from_double_exact(p32_to_double(u[i])) != u[i];
+    return bad;
+}
+// chain_add_run_reg against chain_add_run on one chain of n terms (patterns); 1 on a match
+int hc_chain_reg_check(uint32_t c0, const uint32_t *qp, int n)
+{
+    std::vector<double> q(n > 0 ? n : 1);
+    for (int k = 0; k < n; ++k)
+        q[k] = p32_to_double(qp[k]);
+    const double a = chain_add_run(p32_to_double(c0), q.data(), n);
+    const double b = chain_add_run_reg(p32_to_double(c0), q.data(), n);
+    return p32_from_double(a) == p32_from_double(b);
 }
 // scan_row_emul against chain_add_run on one chain of n terms (patterns); returns 1 on a match
 int hc_scan_row_check(uint32_t c0, const uint32_t *qp, int n, int E, long *stats)

@@ -34,6 +34,9 @@ def hc(tmp_path_factory):
     lib.hc_llt_solve_split.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
     lib.hc_llt_solve_scan.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int, ctypes.c_int, I64]
     lib.hc_scan_row_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int, ctypes.c_int, I64]
+    lib.hc_from_double_exact_mismatch.argtypes = [U32, ctypes.c_long]
+    lib.hc_from_double_exact_mismatch.restype = ctypes.c_long
+    lib.hc_chain_reg_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.restype = ctypes.c_uint32
     lib.hc_f64_add_n.argtypes = [U32, U32, U32, ctypes.c_long]
@@ -306,8 +309,8 @@ def test_fp64_gemm_chains_match_oracle(hc, kind):
 def test_scan_form_of_the_chain_matches_sequential_additions(hc):
     """The scan forms of a chain of additions (step maps M -> M + c[M & 1] on the posit grid
     of the running value's binade, or N -> N + c[N & 3] over two adjacent binades, composed
-    over a warp's window, cut at the first step the form does not cover) equal
-    chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
+    over a warp's window, cut at the first step the form does not cover), and the chain with
+    the rounding constant's regime held fixed over blocks, equal chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
     cancel to zero, hit ties (halves of the grid spacing), span 80 decades, and carry addends
     25..30 binades down."""
     rng = np.random.default_rng(31)
@@ -330,4 +333,18 @@ def test_scan_form_of_the_chain_matches_sequential_additions(hc):
         c0 = int(oracle.from_double(np.array([rng.uniform(-2, 2)]))[0])
         E = int(rng.choice([1, 2, 4, 8, -1, -2, -4, -8]))  # E < 0: the two-binade form
         assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
+        assert hc.hc_chain_reg_check(c0, np.ascontiguousarray(q), n) == 1, (trial, kind, n, "reg")
     assert stats[0] > 0 and stats[1] > 0  # both scans and exact steps were exercised
+
+
+def test_exact_encode_round_trips_every_pattern_class(hc):
+    """p32_from_double_exact (field assembly without rounding, for values that are posits)
+    inverts p32_to_double on random patterns, every regime length and its neighbours,
+    zero, NaR and the extremes."""
+    rng = np.random.default_rng(41)
+    pw = np.array([1 << i for i in range(31)], dtype=np.uint64)
+    edges = np.concatenate([pw, pw - 1, pw + 1, 0x80000000 - pw, 0x80000000 + pw, 0xFFFFFFFF - pw + 1]) % (1 << 32)
+    u = np.concatenate([rng.integers(0, 2**32, 2_000_000, dtype=np.uint64).astype(np.uint32), _mix(rng, 100_000),
+                        edges.astype(np.uint32),
+                        np.array([0, 1, 0x7FFFFFFF, 0x80000000, 0x80000001, 0xFFFFFFFF, 0x40000000], np.uint32)])
+    assert hc.hc_from_double_exact_mismatch(np.ascontiguousarray(u), u.size) == 0
