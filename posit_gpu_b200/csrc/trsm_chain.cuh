@@ -361,135 +361,4 @@ PG_HD double chain_add_run_reg(double t, const double *q, int count)
     return t;
 }
 
-// ---------------------------------------------------------------------------
-// Scan form over two adjacent binades.
-// ---------------------------------------------------------------------------
-// A running sum that hovers near a power of two leaves its binade every few dozen steps,
-// and each exit costs the single-binade form a new window.  So a run covers two binades
-// [2^eL, 2^(eL+2)) instead, in units of the lower binade's spacing v = 2^(eL - fbL):
-// N = |t| / v is an integer in [A, 2A) in the lower binade (A = 2^fbL) and a multiple of
-// r in [2A, 4A) in the upper one, r = 2 (same fraction width) or 1 (the upper binade
-// starts a shorter regime of negative k and has one more fraction bit; spacing unchanged).
-// (Where the upper binade has one fraction bit fewer, r = 4, the other pair is taken.)
-// A step's result is rounded on the grid of the binade the exact sum falls in:
-//   lower (and r == 1): N' = N + K + [F > 1/2] + [F == 1/2] * ((N + K) & 1);
-//   upper, r == 2:      N + K even -> N' = N + K; odd -> N + K + 1 when F > 0, else the
-//                       neighbour of the tie that is 0 mod 4 (the even pattern);
-// so it is N -> N + c[N mod 4], maps that compose.  Which side a step's sum falls on is
-// predicted from a prefix sum of the window's addends (wrong only within rounding noise
-// of 2^(eL+1)), and every step is checked on the true path: a step whose exact sum
-// is on the other side, leaves the pair, starts at the pair's top or is risky ends the run.
-// (The prediction only decides how far a window gets, never a result bit.)
-// The maps' displacements wrap modulo 2^32: only a path that has already taken an
-// invalid step can reach large values, and no value past the first invalid step is used.
-struct Seg2Fn {
-    uint32_t c[4]; // displacement for N mod 4 == 0..3
-};
-
-struct Seg2Params {
-    double w;        // sg * 2^(fbL - eL): q * w is q in units of v, sign-folded
-    double vs;       // sg * 2^(eL - fbL): t = vs * N
-    double rlo, rhi; // |q * w| in [rlo, rhi): 25..30 binades below either binade
-    double mid;      // 2A as a double, the side boundary
-    int32_t A;
-    int32_t N0;
-    uint32_t r2;     // 1 when r == 2
-};
-
-PG_HD int32_t posit_fb(int32_t e)
-{
-    const int32_t k = e >> 2;
-    return 28 - ((k ^ (k >> 31)) + 1);
-}
-
-// false when t is zero, or no pair around its binade lies in the fast window.
-PG_HD bool seg2_begin(double t, Seg2Params &sp)
-{
-    const uint64_t b = f64_bits(t);
-    const int32_t e = (int32_t)((b >> 52) & 0x7FF) - 1023;
-    if (t == 0.0)
-        return false;
-    // the pair that puts t nearer its middle: the upper half of t's binade pairs upward
-    const bool upper_half = (b >> 51) & 1;
-    int32_t eL = upper_half ? e : e - 1;
-    if (posit_fb(eL + 1) < posit_fb(eL)) // r == 4: take the other pair
-        eL = upper_half ? e - 1 : e;
-    if (eL < FAST_LO || eL + 1 > FAST_HI)
-        return false;
-    const int32_t fbL = posit_fb(eL), fbU = posit_fb(eL + 1);
-    const uint32_t neg = (uint32_t)(b >> 63);
-    sp.w = seg_pow2(fbL - eL, neg);
-    sp.vs = seg_pow2(eL - fbL, neg);
-    sp.rlo = seg_pow2(fbL - 30, 0);
-    sp.rhi = seg_pow2(fbL - 23, 0);
-    sp.A = 1 << fbL;
-    sp.mid = (double)(2 << fbL);
-    sp.N0 = (int32_t)(t * sp.w);
-    sp.r2 = fbU == fbL;
-    return true;
-}
-
-// floor(Q) with Q clamped to +-SEG_SAT (an addend that large leaves the pair anyway)
-PG_HD int32_t seg2_floor(double Q)
-{
-    const double Qc = Q > (double)SEG_SAT ? (double)SEG_SAT : (Q < -(double)SEG_SAT ? -(double)SEG_SAT : Q);
-    return (int32_t)floor(Qc);
-}
-
-// The step map of addend Q (in units of v) whose sum is predicted on side `up_side`;
-// K, and the [lo, lo + span) range the exact sum N + K must fall in.
-PG_HD Seg2Fn seg2_fn(double Q, bool up_side, const Seg2Params &sp, int32_t &K, int32_t &lo, int32_t &span)
-{
-    const double aQ = Q < 0 ? -Q : Q;
-    const bool risky = (aQ >= sp.rlo) & (aQ < sp.rhi);
-    const double Qc = Q > (double)SEG_SAT ? (double)SEG_SAT : (Q < -(double)SEG_SAT ? -(double)SEG_SAT : Q);
-    const double Kd = floor(Qc);
-    const double F = Qc - Kd; // exact
-    K = (int32_t)Kd;
-    const uint32_t ku = (uint32_t)K;
-    const uint32_t up = F > 0.5, tie = F == 0.5, fpos = F > 0.0;
-    Seg2Fn f;
-    if (up_side & (sp.r2 != 0)) {
-        // by (N + K) mod 4: 0 -> 0, 1 -> F > 0 ? +1 : -1, 2 -> 0, 3 -> +1
-        const uint32_t d1 = fpos ? 1u : 0xFFFFFFFFu;
-#pragma unroll
-        for (int rho = 0; rho < 4; ++rho) {
-            const uint32_t m = (ku + rho) & 3u;
-            f.c[rho] = ku + (m == 1 ? d1 : (m == 3 ? 1u : 0u));
-        }
-    } else {
-#pragma unroll
-        for (int rho = 0; rho < 4; ++rho)
-            f.c[rho] = ku + (up | (tie & ((ku + rho) & 1u)));
-    }
-    lo = up_side ? 2 * sp.A : sp.A;
-    span = risky ? 0 : (up_side ? 2 * sp.A : sp.A);
-    return f;
-}
-
-PG_HD uint32_t seg2_pick(const Seg2Fn &g, uint32_t i)
-{
-    const uint32_t a = (i & 1) ? g.c[1] : g.c[0];
-    const uint32_t b = (i & 1) ? g.c[3] : g.c[2];
-    return (i & 2) ? b : a;
-}
-
-// g after f
-PG_HD Seg2Fn seg2_then(const Seg2Fn &f, const Seg2Fn &g)
-{
-    Seg2Fn h;
-#pragma unroll
-    for (int rho = 0; rho < 4; ++rho)
-        h.c[rho] = f.c[rho] + seg2_pick(g, (uint32_t)rho + f.c[rho]);
-    return h;
-}
-
-PG_HD int32_t seg2_apply(const Seg2Fn &f, int32_t N) { return (int32_t)((uint32_t)N + seg2_pick(f, (uint32_t)N)); }
-
-// Is the step from N (on the true path, N >= A) exact in the scan form?
-PG_HD bool seg2_valid(int32_t N, int32_t K, int32_t lo, int32_t span, const Seg2Params &sp)
-{
-    return (N < 4 * sp.A) & ((uint32_t)(N + K - lo) < (uint32_t)span);
-}
-
 } // namespace pg

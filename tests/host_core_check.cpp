@@ -268,71 +268,6 @@ static double scan_row_emul(double t, const double *q, int len, int E, long *seg
     return t;
 }
 
-// The two-binade scan form (Seg2*) as lapack.cu's warp_chain_scan runs it: per window,
-// the addends in units of v, the running sum of their integer parts for the side
-// predictions, the lanes' composed maps, their walks from their true starts.
-static double scan_row_emul2(double t, const double *q, int len, int E, long *segs, long *exact)
-{
-    constexpr int LANES = 32;
-    std::vector<Seg2Fn> start(LANES);
-    std::vector<double> Q(LANES * E), P(LANES * E);
-    int pos = 0;
-    while (pos < len) {
-        Seg2Params sp;
-        if (!seg2_begin(t, sp)) {
-            t = chain_add_one(t, q[pos]);
-            ++pos;
-            ++*exact;
-            continue;
-        }
-        ++*segs;
-        const int end = std::min(len, pos + LANES * E);
-        uint32_t run = (uint32_t)sp.N0; // side predictions as lapack.cu makes them
-        for (int j = pos; j < end; ++j) {
-            Q[j - pos] = q[j] * sp.w;
-            run += (uint32_t)seg2_floor(Q[j - pos]);
-            P[j - pos] = (double)(int32_t)run;
-        }
-        Seg2Fn acc = {{0, 0, 0, 0}};
-        for (int l = 0; l < LANES; ++l) {
-            start[l] = acc;
-            Seg2Fn f = {{0, 0, 0, 0}};
-            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
-            for (int j = j0; j < j1; ++j) {
-                int32_t K, lo, span;
-                f = seg2_then(f, seg2_fn(Q[j - pos], P[j - pos] >= sp.mid, sp, K, lo, span));
-            }
-            acc = seg2_then(acc, f);
-        }
-        uint64_t key = ~0ull;
-        int32_t Nend = 0;
-        for (int l = 0; l < LANES; ++l) {
-            const int j0 = pos + l * E, j1 = std::min(j0 + E, end);
-            int32_t N = seg2_apply(start[l], sp.N0);
-            for (int j = j0; j < j1; ++j) {
-                int32_t K, lo, span;
-                const Seg2Fn f = seg2_fn(Q[j - pos], P[j - pos] >= sp.mid, sp, K, lo, span);
-                if (!seg2_valid(N, K, lo, span, sp)) {
-                    key = std::min(key, ((uint64_t)j << 32) | (uint32_t)N);
-                    break;
-                }
-                N = seg2_apply(f, N);
-            }
-            if (j1 == end && j0 < end)
-                Nend = N;
-        }
-        if (key == ~0ull) {
-            t = sp.vs * (double)Nend;
-            pos = end;
-        } else {
-            const int js = (int)(key >> 32);
-            t = chain_add_one(sp.vs * (double)(int32_t)(uint32_t)key, q[js]);
-            pos = js + 1;
-            ++*exact;
-        }
-    }
-    return t;
-}
 // The L^T solve with rows summed by scan_row_emul; stats[0] += scans, stats[1] += exact steps.
 void hc_llt_solve_scan(const uint32_t *L, long ld, uint32_t *b, int m, int E, long *stats)
 {
@@ -343,9 +278,8 @@ void hc_llt_solve_scan(const uint32_t *L, long ld, uint32_t *b, int m, int E, lo
         const int len = m - 1 - i;
         for (int j = 0; j < len; ++j)
             q[j] = llt_term(li[i + 1 + j], b[i + 1 + j], &nar);
-        const double t0 = p32_to_double(b[i] == P32_NAR ? 0u : b[i]);
-        const double c = E > 0 ? scan_row_emul(t0, q.data(), len, E, &stats[0], &stats[1])
-                               : scan_row_emul2(t0, q.data(), len, -E, &stats[0], &stats[1]);
+        const double c = scan_row_emul(p32_to_double(b[i] == P32_NAR ? 0u : b[i]), q.data(), len, E,
+                                       &stats[0], &stats[1]);
         uint32_t t = nar ? P32_NAR : p32_from_double(c);
         b[i] = pdiv(t, li[i]);
     }
@@ -375,8 +309,7 @@ int hc_scan_row_check(uint32_t c0, const uint32_t *qp, int n, int E, long *stats
     for (int k = 0; k < n; ++k)
         q[k] = p32_to_double(qp[k]);
     const double a = chain_add_run(p32_to_double(c0), q.data(), n);
-    const double b = E > 0 ? scan_row_emul(p32_to_double(c0), q.data(), n, E, &stats[0], &stats[1])
-                           : scan_row_emul2(p32_to_double(c0), q.data(), n, -E, &stats[0], &stats[1]);
+    const double b = scan_row_emul(p32_to_double(c0), q.data(), n, E, &stats[0], &stats[1]);
     return p32_from_double(a) == p32_from_double(b);
 }
 }

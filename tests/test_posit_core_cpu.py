@@ -160,7 +160,7 @@ def test_lower_transposed_solve_matches_oracle(hc):
             got = b.copy()
             solve(L, m, got, m)
             assert np.array_equal(got, want), (m, kind, solve.__name__)
-        for E in (1, 4, -1, -8):  # E < 0: the two-binade form
+        for E in (1, 4):
             got = b.copy()
             hc.hc_llt_solve_scan(L, m, got, m, E, np.zeros(2, np.int64))
             assert np.array_equal(got, want), (m, kind, "scan", E)
@@ -307,9 +307,9 @@ def test_fp64_gemm_chains_match_oracle(hc, kind):
 
 
 def test_scan_form_of_the_chain_matches_sequential_additions(hc):
-    """The scan forms of a chain of additions (step maps M -> M + c[M & 1] on the posit grid
-    of the running value's binade, or N -> N + c[N & 3] over two adjacent binades, composed
-    over a warp's window, cut at the first step the form does not cover), and the chain with
+    """The scan form of a chain of additions (step maps M -> M + c[M & 1] on the posit grid
+    of the running value's binade, composed over a warp's window, cut at the first step the
+    form does not cover, short windows followed by sequential runs), and the chain with
     the rounding constant's regime held fixed over blocks, equal chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
     cancel to zero, hit ties (halves of the grid spacing), span 80 decades, and carry addends
     25..30 binades down."""
@@ -331,7 +331,7 @@ def test_scan_form_of_the_chain_matches_sequential_additions(hc):
         else:  # addends 24..31 binades below a running value near 1
             q = oracle.from_double(rng.choice([-1, 1], n) * 2.0 ** -rng.integers(24, 32, n) * rng.uniform(1, 2, n))
         c0 = int(oracle.from_double(np.array([rng.uniform(-2, 2)]))[0])
-        E = int(rng.choice([1, 2, 4, 8, -1, -2, -4, -8]))  # E < 0: the two-binade form
+        E = int(rng.choice([1, 2, 4, 8]))
         assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
         assert hc.hc_chain_reg_check(c0, np.ascontiguousarray(q), n) == 1, (trial, kind, n, "reg")
     assert stats[0] > 0 and stats[1] > 0  # both scans and exact steps were exercised
