@@ -296,7 +296,7 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
 } // namespace
 
 #ifndef PG_BATCH_MIN_CTAS
-#define PG_BATCH_MIN_CTAS 4 // 64 registers: 4 resident CTAs per SM (measured best of 2, 3, 4)
+#define PG_BATCH_MIN_CTAS 6 // 40 registers: 6 resident CTAs per SM (measured best of 2, 3, 4, 6, 8)
 #endif
 __global__ void __launch_bounds__(BT, PG_BATCH_MIN_CTAS) batch_factor_kernel(const BatchProblem *__restrict__ probs, int nprob,
                                                           const int *__restrict__ order, int *__restrict__ next)

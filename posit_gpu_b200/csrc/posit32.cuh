@@ -666,11 +666,11 @@ struct F64ConstComputed {
 //   q = fma(t, a, Cp) - Cp    the exact product rounded once to the posit grid of its
 //                             binade (taken from fl(t*a); where that rounds up to a power
 //                             of two both give that power);
-//   s = c + q, err            the sum and its exact rounding error (TwoSum, Knuth: err =
-//                             e1 + e2 exactly): when err == 0 the FP64 sum is exact;
+//   s = c + q                 the FP64 sum, tested for exactness: s - c == q and s - q == c
+//                             (Fast2Sum on the larger operand makes an inexact s fail it);
 //   r = (s + Cs) - Cs         the exact sum rounded to the posit grid of its binade.
-// Bit 30 of `bad` is set when the step must be done exactly instead: an inexact FP64 sum
-// (err != 0), or a product or sum outside the fast window (its constant is NaN, so r is).
+// Bit 30 of `bad` is set when the step must be done exactly instead: an inexact FP64 sum,
+// or a product or sum outside the fast window (its constant is NaN, so r is).
 // Flagging every inexact sum is conservative: beyond 30 binades the rounded sum would be
 // right anyway, but that case is rare on the data the GEMM sees.
 template <class ConstOf>
@@ -680,12 +680,13 @@ PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, uint3
     const double Cp = f64_from_bits(const_of(f64_binade(p)));
     const double q = f64_add(f64_fma(t, a, Cp), -Cp);
     const double s = f64_add(c, q);
-    // TwoSum's error is e1 + e2 (an exact addition); e1 == -e2 tests it for zero
-    const double bq = f64_add(s, -c);
-    const double e1 = f64_add(c, -f64_add(s, -bq)), e2 = f64_add(q, -bq);
+    // s is exact iff s - c == q and s - q == c: with the operands ordered by exponent,
+    // s - larger is exact (Dekker's Fast2Sum), so an inexact s leaves that difference
+    // unequal to the smaller operand
+    const bool inexact = (f64_add(s, -c) != q) | (f64_add(s, -q) != c);
     const double Cs = f64_from_bits(const_of(f64_binade(s)));
     const double r = f64_add(f64_add(s, Cs), -Cs);
-    const bool fail = (e1 != -e2) | (r != r);
+    const bool fail = inexact | (r != r);
     bad |= fail ? 0x40000000u : 0u;
     return r;
 }
