@@ -82,11 +82,11 @@ __device__ __forceinline__ void tile_steps(dp32 (&acc)[TM_][TN_], const uint2 *a
 
 // The same k-steps in the FP64 form (posit32.cuh, f64_posit_mac): operands and
 // accumulators are posit32 values held in FP64; as = [l][16*TM_] and ts = [l][16*TN_] are
-// FP64 tiles; ctab holds the rounding constant of every FP64 binade.  Failed steps are
+// FP64 tiles; ctab holds the rounding constants (F64ConstTable).  Failed steps are
 // committed branch-free as no-ops and redone afterwards on patterns, in order.
 template <int TM_, int TN_>
 __device__ __forceinline__ void tile_steps_f64(double (&acc)[TM_][TN_], const double *as, const double *ts,
-                                               int lmax, const uint64_t *ctab, int tx, int ty)
+                                               int lmax, const uint32_t *ctab, int tx, int ty)
 {
     constexpr int BM_ = 16 * TM_, BN_ = 16 * TN_;
     const F64ConstTable const_of{ctab};
@@ -109,10 +109,10 @@ __device__ __forceinline__ void tile_steps_f64(double (&acc)[TM_][TN_], const do
         for (int i = 0; i < TM_; ++i) {
 #pragma unroll
             for (int j = 0; j < TN_; ++j) {
-                uint32_t bad = 0;
+                bool bad;
                 const double r = f64_posit_mac(acc[i][j], t[j], a[i], const_of, bad);
                 acc[i][j] = bad ? acc[i][j] : r;
-                fail += __umulhi(bad, 4u << (i * TN_ + j)); // 2^(i*TN_+j) when failed
+                fail += __umulhi(bad ? 0x40000000u : 0u, 4u << (i * TN_ + j)); // 2^(i*TN_+j) when failed
             }
         }
         if (fail) { // rare: redo the failed steps exactly, in the same order

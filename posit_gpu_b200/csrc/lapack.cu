@@ -212,12 +212,7 @@ __global__ void laswp_kernel(uint32_t *__restrict__ A, size_t lda, int ncols, in
 // b_i - b_k*a_ik is the FP64 multiply-add step of the GEMM (posit32.cuh, f64_posit_mac),
 // its rare flagged steps redone on patterns.  NaR travels as NaN (every step that meets
 // it is flagged and redone on patterns, which give NaR).
-PG_HD double trsm_update(double c, double t, double a)
-{
-    uint32_t bad = 0;
-    const double r = f64_posit_mac(c, t, a, F64ConstComputed{}, bad);
-    return (bad & 0x40000000u) ? f64_posit_mac_exact(c, t, a) : r;
-}
+PG_HD double trsm_update(double c, double t, double a) { return f64_posit_mac_checked(c, t, a); }
 
 // The column: staged in shared memory as FP64, or (too long for that) left in place as
 // patterns and converted at every access.

@@ -642,23 +642,46 @@ PG_HD bool f64_outside_fast(int32_t eb)
 // Biased FP64 exponent field (the binade) of x.
 PG_HD int32_t f64_binade(double x) { return (int32_t)((f64_bits(x) >> 52) & 0x7FF); }
 
-// The rounding constant for binade `eb` as FP64 bits: C = 1.5 * 2^(e + 52 - fb).  A binade
+// High and low 32-bit words of an FP64 value, and an FP64 value from its high word (low
+// word 0: every rounding constant is one).
+PG_HD uint32_t f64_hi(double x)
+{
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__double2hiint(x);
+#else
+    return (uint32_t)(f64_bits(x) >> 32);
+#endif
+}
+PG_HD double f64_from_hi(uint32_t h)
+{
+#if defined(__CUDA_ARCH__)
+    return __hiloint2double((int)h, 0);
+#else
+    return f64_from_bits((uint64_t)h << 32);
+#endif
+}
+
+// The rounding constant's high word for an FP64 value whose top 12 bits (sign and
+// exponent field) are `top`: C = 1.5 * 2^(e + 52 - fb), the same for either sign.  A binade
 // outside the fast window gets a NaN instead, so that a product or sum falling there comes
 // out NaN and is redone exactly.  Binade 0 holds zero (a zero product or an exactly
 // cancelling sum): in the window.
-PG_HD uint64_t f64_round_const(int32_t eb)
+PG_HD uint32_t f64_round_const_top(uint32_t top)
 {
+    const int32_t eb = (int32_t)(top & 0x7FF);
     if (eb != 0 && f64_outside_fast(eb))
-        return 0x7FF8000000000000ull;
-    return (uint64_t)f64_round_const_hi(eb) << 32;
+        return 0x7FF80000u;
+    return f64_round_const_hi(eb);
 }
-constexpr int F64_BINADES = 2048; // FP64 exponent fields
+// The table the GEMM kernels keep in shared memory: f64_round_const_top for every top
+// 12 bits, so that a lookup is one shift of the value's high word.
+constexpr int F64_CONST_ENTRIES = 4096;
 struct F64ConstTable {
-    const uint64_t *tab; // f64_round_const for every binade 0..2047
-    PG_HD_MEMBER uint64_t operator()(int32_t eb) const { return tab[eb]; }
+    const uint32_t *tab;
+    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(tab[f64_hi(x) >> 20]); }
 };
 struct F64ConstComputed {
-    PG_HD_MEMBER uint64_t operator()(int32_t eb) const { return f64_round_const(eb); }
+    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(f64_round_const_top(f64_hi(x) >> 20)); }
 };
 
 // c + t*a with both roundings (p32_mul, kernel_entry.cl:399-538, then p32_add,
@@ -669,25 +692,24 @@ struct F64ConstComputed {
 //   s = c + q                 the FP64 sum, tested for exactness: s - c == q and s - q == c
 //                             (Fast2Sum on the larger operand makes an inexact s fail it);
 //   r = (s + Cs) - Cs         the exact sum rounded to the posit grid of its binade.
-// Bit 30 of `bad` is set when the step must be done exactly instead: an inexact FP64 sum,
-// or a product or sum outside the fast window (its constant is NaN, so r is).
+// `fail` is set when the step must be done exactly instead: an inexact FP64 sum, or a
+// product or sum outside the fast window (its constant is NaN, so r is).
 // Flagging every inexact sum is conservative: beyond 30 binades the rounded sum would be
 // right anyway, but that case is rare on the data the GEMM sees.
 template <class ConstOf>
-PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, uint32_t &bad)
+PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, bool &fail)
 {
     const double p = f64_mul(t, a);
-    const double Cp = f64_from_bits(const_of(f64_binade(p)));
+    const double Cp = const_of(p);
     const double q = f64_add(f64_fma(t, a, Cp), -Cp);
     const double s = f64_add(c, q);
     // s is exact iff s - c == q and s - q == c: with the operands ordered by exponent,
     // s - larger is exact (Dekker's Fast2Sum), so an inexact s leaves that difference
     // unequal to the smaller operand
     const bool inexact = (f64_add(s, -c) != q) | (f64_add(s, -q) != c);
-    const double Cs = f64_from_bits(const_of(f64_binade(s)));
+    const double Cs = const_of(s);
     const double r = f64_add(f64_add(s, Cs), -Cs);
-    const bool fail = inexact | (r != r);
-    bad |= fail ? 0x40000000u : 0u;
+    fail = inexact | (r != r);
     return r;
 }
 
@@ -701,9 +723,9 @@ PG_HD double f64_posit_mac_exact(double c, double t, double a)
 // c + t*a with the exact path taken where the FP64 step is flagged.
 PG_HD double f64_posit_mac_checked(double c, double t, double a)
 {
-    uint32_t bad = 0;
-    const double r = f64_posit_mac(c, t, a, F64ConstComputed{}, bad);
-    return (bad & 0x40000000u) ? f64_posit_mac_exact(c, t, a) : r;
+    bool fail;
+    const double r = f64_posit_mac(c, t, a, F64ConstComputed{}, fail);
+    return fail ? f64_posit_mac_exact(c, t, a) : r;
 }
 
 // FP64 -> posit32 for a value that IS a posit32 value (an output of the FP64 steps or of

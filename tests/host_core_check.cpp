@@ -125,11 +125,15 @@ long hc_f64_add_n(const uint32_t *t, const uint32_t *q, uint32_t *o, long n)
 // c + t*a through the FP64 step (with its exact fallback) on n triples, the rounding
 // constants from a table (use_table) or computed; returns the number of steps handed to
 // the exact path.  NaR operands are handled outside (flags) by the GEMM.
-static uint64_t g_ctab[2048];
+static uint32_t g_ctab[F64_CONST_ENTRIES];
+static void fill_ctab()
+{
+    for (int e = 0; e < F64_CONST_ENTRIES; e++)
+        g_ctab[e] = f64_round_const_top((uint32_t)e);
+}
 long hc_f64_mac_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, uint32_t *o, long n, int use_table)
 {
-    for (int e = 0; e < 2048; e++)
-        g_ctab[e] = f64_round_const(e);
+    fill_ctab();
     long flagged = 0;
     for (long i = 0; i < n; i++) {
         if (c[i] == P32_NAR || t[i] == P32_NAR || a[i] == P32_NAR) {
@@ -137,11 +141,11 @@ long hc_f64_mac_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, uint3
             continue;
         }
         const double dc = p32_to_double(c[i]), dt = p32_to_double(t[i]), da = p32_to_double(a[i]);
-        uint32_t bad = 0;
+        bool bad;
         const double r = use_table ? f64_posit_mac(dc, dt, da, F64ConstTable{g_ctab}, bad)
                                    : f64_posit_mac(dc, dt, da, F64ConstComputed{}, bad);
-        flagged += (bad & 0x40000000u) != 0;
-        o[i] = p32_from_double((bad & 0x40000000u) ? f64_posit_mac_exact(dc, dt, da) : r);
+        flagged += bad;
+        o[i] = p32_from_double(bad ? f64_posit_mac_exact(dc, dt, da) : r);
     }
     return flagged;
 }
@@ -177,14 +181,13 @@ long hc_find_tie_products(uint64_t seed, long tries, uint32_t *t_out, uint32_t *
 // the table, exact fixups), as the kernels run them; returns the number of fixups
 long hc_f64_gemm_chains(const uint32_t *c0, const uint32_t *t, const uint32_t *a, uint32_t *o, long nchains, long len)
 {
-    for (int e = 0; e < 2048; e++)
-        g_ctab[e] = f64_round_const(e);
+    fill_ctab();
     long fixes = 0;
     for (long j = 0; j < nchains; j++) {
         double c = p32_to_double(c0[j]);
         for (long l = 0; l < len; l++) {
             const double dt = p32_to_double(t[j * len + l]), da = p32_to_double(a[j * len + l]);
-            uint32_t bad = 0;
+            bool bad;
             const double r = f64_posit_mac(c, dt, da, F64ConstTable{g_ctab}, bad);
             if (bad) {
                 c = f64_posit_mac_exact(c, dt, da);
