@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--trans", default="NN")
+    ap.add_argument("--trailing", type=int, default=0,
+                    help="gemm: the LU trailing-update shape m = n = N-b, k = b (b = this value, N = --n)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="gemm", choices=["gemm", "lu", "cholesky", "batch", "serve"],
@@ -69,12 +71,21 @@ def parse():
     return ap.parse_args()
 
 
+def shape(args):
+    """(m, n, k) of the GEMM arm: N^3, or the trailing-update shape (N-b) x (N-b) x b."""
+    if args.trailing:
+        return args.n - args.trailing, args.n - args.trailing, args.trailing
+    return args.n, args.n, args.n
+
+
 def config(args):
-    n = args.n
-    return {"workload": f"posit32 Rgemm {args.trans} {n}^3, alpha=-1, beta=1, U[-1,1], column-major, ld={n}",
-            "m": n, "n": n, "k": n, "transa": args.trans[0], "transb": args.trans[1],
-            "alpha": "-1", "beta": "1", "dist": "uniform[-1,1] (seeded FP64 -> posit32)",
-            "l2": "inputs larger than L2 (A, B, C 4*n^2 bytes each + 8*(m+n)*k-byte decoded workspace)",
+    m, n, k = shape(args)
+    what = (f"{m}x{n}x{k} (LU trailing update of {args.n}, b={k})" if args.trailing else f"{n}^3")
+    l2 = ("inputs larger than L2 (A, B, C 4*n^2 bytes each + 8*(m+n)*k-byte decoded workspace)"
+          if not args.trailing else "C (4*m*n bytes) larger than L2")
+    return {"workload": f"posit32 Rgemm {args.trans} {what}, alpha=-1, beta=1, U[-1,1], column-major",
+            "m": m, "n": n, "k": k, "transa": args.trans[0], "transb": args.trans[1],
+            "alpha": "-1", "beta": "1", "dist": "uniform[-1,1] (seeded FP64 -> posit32)", "l2": l2,
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
@@ -220,8 +231,10 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
     pg.init()
-    n = args.n
+    m, n, k = shape(args)
     ta, tb = args.trans[0], args.trans[1]
+    lda = m if ta in "nN" else k
+    ldb = k if tb in "nN" else n
     alpha, beta = pg.P32_MINUS_ONE, pg.P32_ONE
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
@@ -230,14 +243,14 @@ def ours(args):
         x = torch.rand(numel, dtype=torch.float64, device=dev, generator=g) * 2.0 - 1.0
         return pg.from_double_dev(x)
 
-    A = rand_posit(n * n)
-    B = rand_posit(n * n)
-    C = rand_posit(n * n)
-    ws = torch.empty(pg.workspace_size(ta, tb, n, n, n), dtype=torch.uint8, device=dev)
+    A = rand_posit(m * k)
+    B = rand_posit(k * n)
+    C = rand_posit(m * n)
+    ws = torch.empty(pg.workspace_size(ta, tb, m, n, k), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step():
-        pg.Rgemm_dev(ta, tb, n, n, n, alpha, A, n, B, n, beta, C, n, workspace=ws, stream=stream)
+        pg.Rgemm_dev(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, m, workspace=ws, stream=stream)
 
     for _ in range(args.warmup):
         step()
@@ -272,11 +285,11 @@ def ours(args):
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    ops_per_step = 2.0 * n * n * n
+    ops_per_step = 2.0 * m * n * k
     value = world * ops_per_step * args.steps / (ms_max / 1e3) / 1e9
 
     # roofline of the main kernel: instruction issue (FP64 pipe the busiest pipe)
-    mads = float(n) * n * n
+    mads = float(m) * n * k
     main_avg_s = main_ms / 1e3 / max(main_launches, 1) if main_launches else 0.0
     sm_mhz = clocks.get("sm_mhz") or perf.SM_MAX_MHZ
     peak = perf.issue_peak_warp_inst_per_s(sm_mhz)
@@ -298,6 +311,21 @@ def ours(args):
                               "MEASURED_PEAKS.json has no issue or FP64 figure",
                 "inst_source": perf.INST_SOURCE}
 
+    if args.trailing:
+        # short k: HBM reported beside the issue roofline (algorithmic bytes 4*(mk + kn + 2mn))
+        alg = 4.0 * (m * k + k * n + 2.0 * m * n)
+        step_s = ms_max / args.steps / 1e3
+        peak_gbs = None
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                peak_gbs = json.load(fh).get("hbm_gbs")
+        except (OSError, ValueError):
+            pass
+        roofline["hbm"] = {"algorithmic_bytes": alg, "achieved_gbs": round(alg / step_s / 1e9, 1),
+                           "peak_gbs": peak_gbs,
+                           "frac": peak_gbs and round(alg / step_s / 1e9 / peak_gbs, 4),
+                           "peak_basis": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"}
+
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "posit32",
@@ -310,25 +338,25 @@ def ours(args):
         hB = B.cpu().pin_memory()
         hC = C.cpu().pin_memory()
         nA, nB, nC = hA.numpy(), hB.numpy(), hC.numpy()
-        pg.Rgemm(ta, tb, n, n, n, alpha, nA, n, nB, n, beta, nC, n)  # warm
+        pg.Rgemm(ta, tb, m, n, k, alpha, nA, lda, nB, ldb, beta, nC, m)  # warm
         if dist:
             dist.barrier()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         esteps = max(1, min(args.steps, 3))
         for _ in range(esteps):
-            pg.Rgemm(ta, tb, n, n, n, alpha, nA, n, nB, n, beta, nC, n)
+            pg.Rgemm(ta, tb, m, n, k, alpha, nA, lda, nB, ldb, beta, nC, m)
         e2e_s = time.perf_counter() - t0
         te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         if dist:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e_s = float(te.item())
         line["e2e"] = {"value": round(world * ops_per_step * esteps / e2e_s / 1e9, 3), "unit": UNIT,
-                       "h2d_bytes_per_step": 3 * 4 * n * n, "d2h_bytes_per_step": 4 * n * n,
+                       "h2d_bytes_per_step": 4 * (m * k + k * n + m * n), "d2h_bytes_per_step": 4 * m * n,
                        "steps": esteps, "timing": "host wall clock around the synchronous call"}
 
     # CPU baseline: the reference's own Rgemm on a column slice, rank 0, N = 1 only
-    if world == 1 and not args.no_cpu:
+    if world == 1 and not args.no_cpu and not args.trailing:
         try:
             import oracle
             threads = oracle.orc.orc_num_threads()
@@ -417,6 +445,31 @@ def factor_arm(args):
     solve_ms = e0.elapsed_time(e1)
     work = (2.0 if lu else 1.0) / 3.0 * n ** 3
     rep = accuracy.solve_report(A0, b, rhs, x_true=x, n=n, spd=not lu)
+    cpu = None
+    if not args.no_cpu:
+        # the reference's own CPU Rgetrf / Rpotrf (oracle/_ref), full factorization of the
+        # leading block of the same matrix (same distribution), same nb
+        try:
+            import numpy as np
+
+            import oracle
+            nc = min(n, 1024)
+            blk = A0.view(n, n).t()[:nc, :nc].t().contiguous().cpu().numpy().view(np.uint32).reshape(-1).copy()
+            piv = np.zeros(nc, dtype=np.int32)
+            t0 = time.perf_counter()
+            if oracle.ref is not None:
+                kind = "reference"
+                (oracle.ref.ref_rgetrf(nc, nc, blk, nc, piv, nb) if lu else oracle.ref.ref_rpotrf(b"L", nc, blk, nc, nb))
+            else:
+                kind = "port"
+                (oracle.orc.orc_rgetrf(nc, nc, blk, nc, piv, nb) if lu else oracle.orc.orc_rpotrf(b"L", nc, blk, nc, nb))
+            dt = time.perf_counter() - t0
+            cwork = (2.0 if lu else 1.0) / 3.0 * nc ** 3
+            cpu = {"value": round(cwork / dt / 1e9, 4), "unit": "Gop/s", "cores": oracle.orc.orc_num_threads(),
+                   "kind": kind, "sample": f"full {'Rgetrf' if lu else 'Rpotrf(L)'} of the leading {nc}x{nc} block "
+                                           f"of the same matrix, nb={nb}, {dt:.1f} s"}
+        except Exception as exc:  # reported, never required
+            cpu = {"value": None, "unit": "Gop/s", "cores": None, "kind": "reference", "sample": f"unavailable: {exc}"}
     line = {"metric": f"posit32 {'Rgetrf' if lu else 'Rpotrf(L)'} Gop/s ({'2/3' if lu else '1/3'} n^3 / t), "
                       f"device-resident, bit-exact vs CPU", "value": round(work / (ms / 1e3) / 1e9, 3),
             "unit": "Gop/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
@@ -425,6 +478,8 @@ def factor_arm(args):
                                                         f"{'U[-1,1]' if lu else 'M*M^T/n + I, M ~ U[-1,1]'}, "
                                                         "one right-hand side b = A*x_true"},
             "info": int(info.item()), "solve_ms": round(solve_ms, 3), "fp64_report": rep}
+    if cpu:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict
 }
 
 // The same solve split over warps (one block per right-hand side, column length m with
-// 20*m bytes of shared memory).  Warp 0 sums row i -- its first term itself, then the
+// 20*m bytes of shared memory for FP64 terms, 12*m for pattern terms).  Warp 0 sums row i -- its first term itself, then the
 // rest in windows of 32*LLT_SCAN_E terms, each summed as one scan over the warp
 // (trsm_chain.cuh, scan form) and cut short at the first step the scan form does not
 // cover, from where one exact step and the next window go on -- while warps
@@ -383,8 +383,8 @@ constexpr int LLT_SEQ_STEPS = 32;    // ... is followed by this many sequential 
 // at the first step the form does not cover (the running value leaves its binade, the
 // step is risky), which is done exactly before the next window starts.  Where windows
 // keep ending early, short runs of sequential steps (chain_add_run_reg) go in between.
-template <int E>
-__device__ double warp_chain_scan(double t, const double *q, int pos, int end)
+template <int E, class Q>
+__device__ double warp_chain_scan(double t, Q q, int pos, int end)
 {
     constexpr unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
@@ -458,12 +458,27 @@ __device__ double warp_chain_scan(double t, const double *q, int pos, int end)
     return t;
 }
 
+// Term storage: FP64, or (for long columns) the posit32 patterns of the products.
+template <class T>
+struct LltTerms;
+template <>
+struct LltTerms<double> {
+    using View = TermsF64;
+    __device__ static double store(uint32_t p) { return p32_to_double(p); }
+};
+template <>
+struct LltTerms<uint32_t> {
+    using View = TermsP32;
+    __device__ static uint32_t store(uint32_t p) { return p; }
+};
+
+template <class T>
 __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint32_t *__restrict__ L, size_t ldl,
                                                                      uint32_t *__restrict__ B, size_t ldb, int m,
                                                                      bool unit, const int *__restrict__ info)
 {
     extern __shared__ __align__(16) unsigned char smem_pc[];
-    double *s_q = reinterpret_cast<double *>(smem_pc); // [2][m]: terms, FP64
+    T *s_q = reinterpret_cast<T *>(smem_pc); // [2][m]: terms
     uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
     __shared__ uint32_t s_nar[2];
     if (info && *info < 0)
@@ -485,7 +500,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
             double c = p32_to_double(bi == P32_NAR ? 0u : bi);
             if (i + 1 < m) {
                 c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
-                c = warp_chain_scan<LLT_SCAN_E>(c, s_q + (size_t)cur * m, i + 2, m);
+                c = warp_chain_scan<LLT_SCAN_E>(c, typename LltTerms<T>::View{s_q + (size_t)cur * m}, i + 2, m);
             }
             uint32_t t = nar ? P32_NAR : p32_from_double(c);
             if (!unit)
@@ -499,10 +514,13 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
         } else if (i >= 1) {
             // terms k = i+1 .. m-1 of row i-1 (their b_k are final)
             const uint32_t *lp = L + (size_t)(i - 1) * ldl;
-            double *qn = s_q + (size_t)(cur ^ 1) * m;
+            T *qn = s_q + (size_t)(cur ^ 1) * m;
             uint32_t nar = 0;
-            for (int k = i + 1 + (tid - 32); k < m; k += LLT_PC_THREADS - 32)
-                qn[k] = llt_term(lp[k], s_b[k], &nar);
+            for (int k = i + 1 + (tid - 32); k < m; k += LLT_PC_THREADS - 32) {
+                const uint32_t p = pmul(0u - s_b[k], lp[k]); // (-b)*a == -(a*b) bit for bit
+                nar |= p == P32_NAR;
+                qn[k] = LltTerms<T>::store(p == P32_NAR ? 0u : p);
+            }
             if (nar)
                 s_nar[cur ^ 1] = 1;
         }
@@ -512,7 +530,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
         bcol[k] = s_b[k];
 }
 
-size_t llt_pc_smem_bytes(int m) { return (size_t)m * (2 * sizeof(double) + 4); }
+size_t llt_pc_smem_bytes(int m, size_t term_bytes) { return (size_t)m * (2 * term_bytes + 4); }
 
 // ---------------------------------------------------------------------------
 // Cholesky panel (lower)
@@ -718,14 +736,22 @@ cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uin
     cudaError_t e = launch_lln(nrhs, threads, A, lda, B, ldb, n, false, nullptr, st);
     if (e != cudaSuccess)
         return e;
-    const size_t pc = llt_pc_smem_bytes(n);
-    if (pc <= (size_t)LLT_SMEM_MAX) {
+    // terms in FP64 where 20n bytes fit, as patterns where 12n bytes do
+    const size_t pc8 = llt_pc_smem_bytes(n, sizeof(double)), pc4 = llt_pc_smem_bytes(n, sizeof(uint32_t));
+    if (pc8 <= (size_t)LLT_SMEM_MAX || pc4 <= (size_t)LLT_SMEM_MAX) {
+        const bool f64 = pc8 <= (size_t)LLT_SMEM_MAX;
+        const size_t pc = f64 ? pc8 : pc4;
         if (pc > 48 * 1024) {
-            e = cudaFuncSetAttribute(trsm_llt_pc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc);
+            e = f64 ? cudaFuncSetAttribute(trsm_llt_pc_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc)
+                    : cudaFuncSetAttribute(trsm_llt_pc_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)pc);
             if (e != cudaSuccess)
                 return e;
         }
-        trsm_llt_pc_kernel<<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
+        if (f64)
+            trsm_llt_pc_kernel<double><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
+        else
+            trsm_llt_pc_kernel<uint32_t><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
         return cudaGetLastError();
     }
     const size_t col = (size_t)n * 4;

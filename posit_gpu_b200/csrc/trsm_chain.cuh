@@ -147,8 +147,10 @@ PG_HD double llt_term(uint32_t l, uint32_t bk, uint32_t *nar)
 }
 
 // t + q_0 + q_1 + ... + q_{count-1}, every addition rounded (p32_add), in that order; t
-// and the q are posit32 values in FP64.  Blocks of CHAIN_BLOCK steps without a branch, the
-// flags tested once per block, a flagged block replayed exactly from its start.
+// and the q are posit32 values in FP64.  (The kernels use the scan form and
+// chain_add_run_reg below; this plain form is the sequence the tests hold them to.)
+// Blocks of CHAIN_BLOCK steps without a branch, the flags tested once per block, a
+// flagged block replayed exactly from its start.
 PG_HD double chain_add_run(double t, const double *q, int count)
 {
     constexpr int U = CHAIN_BLOCK;
@@ -333,7 +335,20 @@ PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint3
 
 // t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-regime step: blocks of
 // CHAIN_BLOCK steps without a branch, a flagged block redone step by step exactly.
-PG_HD double chain_add_run_reg(double t, const double *q, int count)
+// Terms read from FP64 values or from posit32 patterns (converted on load).
+struct TermsF64 {
+    const double *q;
+    PG_HD_MEMBER double operator[](int i) const { return q[i]; }
+    PG_HD_MEMBER TermsF64 operator+(int i) const { return TermsF64{q + i}; }
+};
+struct TermsP32 {
+    const uint32_t *q;
+    PG_HD_MEMBER double operator[](int i) const { return p32_to_double(q[i]); }
+    PG_HD_MEMBER TermsP32 operator+(int i) const { return TermsP32{q + i}; }
+};
+
+template <class Q>
+PG_HD double chain_add_run_reg(double t, Q q, int count)
 {
     constexpr int U = CHAIN_BLOCK;
     int k = 0;
@@ -350,10 +365,10 @@ PG_HD double chain_add_run_reg(double t, const double *q, int count)
 #pragma unroll
         for (int j = 0; j < U; ++j)
             t = f64_posit_add_reg(t, v[j], G, kreg, bad);
-        if (bad & 0x40000000u) {
+        if (bad & 0x40000000u) { // (from q: a dynamic index into v would put v in local memory)
             t = t0;
             for (int j = 0; j < U; ++j)
-                t = chain_add_one(t, v[j]);
+                t = chain_add_one(t, q[k + j]);
         }
     }
     for (; k < count; ++k)

@@ -102,12 +102,13 @@ def test_rpotrs_bit_exact(cuda_ok, n, nrhs):
     assert np.array_equal(g, o)
 
 
-@pytest.mark.parametrize("n,kind", [(300, "wide"), (700, "ties"), (1500, "u")])
+@pytest.mark.parametrize("n,kind", [(300, "wide"), (700, "ties"), (1500, "u"), (11600, "u")])
 def test_rpotrs_any_factor_bit_exact(cuda_ok, n, kind):
     """Rpotrs on lower triangles that are no Cholesky factor: entries over 40 decades, or
     powers of two that make the running sums hit grid ties, zeros in the right-hand sides,
     a NaR in one column -- the transposed solve's chain leaves its binade, cancels and
-    takes the exact path often."""
+    takes the exact path often.  n = 11600 is past the FP64 term buffers' shared-memory
+    limit: the terms are kept as posit patterns."""
     import posit_gpu_b200 as pg
     rng = np.random.default_rng(n)
     if kind == "wide":
@@ -119,7 +120,7 @@ def test_rpotrs_any_factor_bit_exact(cuda_ok, n, kind):
     Lf = np.tril(Lf)
     np.fill_diagonal(Lf, 1.0 + rng.uniform(0, 1, n))
     L = oracle.from_double(Lf.reshape(-1, order="F"))
-    nrhs = 3
+    nrhs = 3 if n < 5000 else 1
     B = oracle.from_double(rng.uniform(-1, 1, n * nrhs))
     B[::7] = 0
     if kind == "wide":
