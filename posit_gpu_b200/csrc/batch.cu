@@ -84,234 +84,6 @@ __device__ int iramax_block(const uint32_t *col, int k, int n, int32_t *s_key, i
     return p;
 }
 
-// iRamax over rows [k, n) of `col` (iRamax.cpp:65-71: the first index of the largest
-// |x| in posit order, NaR lowest), with warp shuffles: two barriers.  s_key/s_idx hold
-// one entry per warp plus the result.
-__device__ int iramax_warp(const uint32_t *col, int k, int n, int32_t *s_key, int *s_idx)
-{
-    constexpr unsigned FULL = 0xFFFFFFFFu;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int32_t best = INT32_MIN;
-    int bidx = n; // n: no row
-    for (int i = k + tid; i < n; i += BT) {
-        const int32_t key = (int32_t)pabs(col[i]);
-        if (bidx == n || key > best) { // rows ascend: the first of equal keys stays
-            best = key;
-            bidx = i;
-        }
-    }
-#pragma unroll
-    for (int round = 0; round < 2; ++round) {
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) { // larger key wins, equal keys: smaller row
-            const int32_t k2 = __shfl_down_sync(FULL, best, off);
-            const int i2 = __shfl_down_sync(FULL, bidx, off);
-            if (i2 < n && (bidx == n || k2 > best || (k2 == best && i2 < bidx))) {
-                best = k2;
-                bidx = i2;
-            }
-        }
-        if (round == 0) {
-            if (lane == 0) {
-                s_key[warp] = best;
-                s_idx[warp] = bidx;
-            }
-            __syncthreads();
-            best = lane < BT / 32 ? s_key[lane] : INT32_MIN;
-            bidx = lane < BT / 32 ? s_idx[lane] : n;
-        }
-    }
-    if (tid == 0)
-        s_idx[BT / 32] = bidx;
-    __syncthreads();
-    return s_idx[BT / 32];
-}
-
-// Blocked right-looking factorizations for n <= BLOCKED_MAX_N: panels of BR columns.
-// Every element still receives its updates a <- a + (-u_kc)*l_ik one at a time in
-// ascending k (the reference's order, see lapack.cu), so the bits are those of the
-// unblocked loop; but a trailing element is loaded, converted and stored once per
-// panel instead of once per column, and the barriers are per panel step.  Staging: the
-// panel's U12 (LU) or L21 (Cholesky) rows as FP64, (n - BR) * BR doubles in s_u.
-constexpr int BR = 4;
-constexpr int BLOCKED_MAX_N = STAGE_DOUBLES / BR;
-
-__device__ __forceinline__ double mac(double c, double t, double a) { return f64_posit_mac_checked(c, t, a); }
-
-// Rgetrf on A (n x n): pivots to ipiv (1-based), returns info.
-__device__ int lu_factor_blocked(const BatchProblem &pr, int32_t *s_key, int *s_idx, double *s_u)
-{
-    const int n = pr.n, tid = threadIdx.x;
-    uint32_t *A = pr.A;
-    const size_t lda = (size_t)pr.lda;
-    __shared__ uint32_t s_piv, s_recip;
-    __shared__ int s_mode;
-    int info = 0;
-    for (int kb = 0; kb < n; kb += BR) {
-        const int jb = min(BR, n - kb), pe = kb + jb; // panel columns [kb, pe)
-        // (1) the panel, column by column
-        for (int k = kb; k < pe; ++k) {
-            uint32_t *ck = A + (size_t)k * lda;
-            const int p = iramax_warp(ck, k, n, s_key, s_idx);
-            const uint32_t piv = ck[p];
-            if (tid == 0) {
-                pr.ipiv[k] = p + 1;
-                if (piv == 0) {
-                    s_mode = 0;
-                } else if ((int32_t)pabs(piv) >= 1) { // Rgetrf2.cpp:103, 121-127
-                    s_mode = 1;
-                    s_recip = pdiv(P32_ONE, piv);
-                } else {
-                    s_mode = 2;
-                }
-                s_piv = piv;
-            }
-            if (piv == 0 && info == 0)
-                info = k + 1;
-            __syncthreads();
-            if (piv != 0 && p != k) // interchange whole rows (Rlaswp on both sides)
-                for (int c = tid; c < n; c += BT) {
-                    uint32_t *pc = A + (size_t)c * lda;
-                    const uint32_t t = pc[k];
-                    pc[k] = pc[p];
-                    pc[p] = t;
-                }
-            __syncthreads();
-            const int mode = s_mode;
-            // scale column k and update the panel's later columns in the same pass
-            double u[BR];
-#pragma unroll
-            for (int c = 0; c < BR; ++c)
-                u[c] = k + 1 + c < pe ? -pd(A[k + (size_t)(k + 1 + c) * lda]) : 0.0;
-            for (int i = k + 1 + tid; i < n; i += BT) {
-                uint32_t l = ck[i];
-                if (mode == 1)
-                    l = pmul(s_recip, l);
-                else if (mode == 2)
-                    l = pdiv(l, s_piv);
-                ck[i] = l;
-                const double dl = pd(l);
-#pragma unroll
-                for (int c = 0; c < BR; ++c)
-                    if (k + 1 + c < pe)
-                        mac_store(A + i + (size_t)(k + 1 + c) * lda, u[c], dl);
-            }
-            __syncthreads();
-        }
-        if (pe >= n)
-            break;
-        // (2) U12: rows [kb, pe) of the trailing columns, unit-lower solve with L11
-        const int nc = n - pe;
-        for (int c = pe + tid; c < n; c += BT) {
-            uint32_t *ac = A + (size_t)c * lda;
-            double u[BR];
-#pragma unroll
-            for (int r = 0; r < BR; ++r) {
-                if (r < jb) {
-                    double v = pd(ac[kb + r]);
-                    for (int k = 0; k < r; ++k)
-                        v = mac(v, -u[k], pd(A[kb + r + (size_t)(kb + k) * lda]));
-                    u[r] = v;
-                    ac[kb + r] = p32_from_double_exact(v);
-                    s_u[(c - pe) * BR + r] = -v;
-                }
-            }
-        }
-        __syncthreads();
-        // (3) the trailing block: a_ic += (-u_kc)*l_ik, k = kb .. pe-1 in order; a thread
-        // keeps its row's l_ik in registers and walks the columns
-        for (int i = pe + tid; i < n; i += BT) {
-            double l[BR];
-#pragma unroll
-            for (int k = 0; k < BR; ++k)
-                l[k] = k < jb ? pd(A[i + (size_t)(kb + k) * lda]) : 0.0;
-            for (int c = 0; c < nc; ++c) {
-                uint32_t *pa = A + i + (size_t)(pe + c) * lda;
-                double a = pd(*pa);
-#pragma unroll
-                for (int k = 0; k < BR; ++k)
-                    if (k < jb)
-                        a = mac(a, s_u[c * BR + k], l[k]);
-                *pa = p32_from_double_exact(a);
-            }
-        }
-        __syncthreads();
-    }
-    return info;
-}
-
-// Rpotrf('L') on A (n x n), returns info.
-__device__ int chol_factor_blocked(const BatchProblem &pr, double *s_u)
-{
-    const int n = pr.n, tid = threadIdx.x;
-    uint32_t *A = pr.A;
-    const size_t lda = (size_t)pr.lda;
-    __shared__ uint32_t s_recip;
-    __shared__ int s_fail;
-    for (int kb = 0; kb < n; kb += BR) {
-        const int jb = min(BR, n - kb), pe = kb + jb;
-        // (1) the panel: diagonal (Rpotrf2.cpp:97), scaling (Rtrsm.cpp:265-268), and the
-        // panel's later columns
-        for (int k = kb; k < pe; ++k) {
-            uint32_t *ck = A + (size_t)k * lda;
-            if (tid == 0) {
-                const uint32_t akk = ck[k];
-                s_fail = (int32_t)akk <= 0;
-                if (!s_fail) {
-                    const uint32_t lkk = psqrt(akk);
-                    ck[k] = lkk;
-                    s_recip = pdiv(P32_ONE, lkk);
-                }
-            }
-            __syncthreads();
-            if (s_fail)
-                return k + 1;
-            for (int i = k + 1 + tid; i < n; i += BT)
-                ck[i] = pmul(s_recip, ck[i]);
-            __syncthreads();
-            double lc[BR];
-#pragma unroll
-            for (int c = 0; c < BR; ++c)
-                lc[c] = k + 1 + c < pe ? -pd(ck[k + 1 + c]) : 0.0;
-            for (int i = k + 1 + tid; i < n; i += BT) {
-                const double li = pd(ck[i]);
-#pragma unroll
-                for (int c = 0; c < BR; ++c)
-                    if (k + 1 + c < pe && i >= k + 1 + c)
-                        mac_store(A + i + (size_t)(k + 1 + c) * lda, lc[c], li);
-            }
-            __syncthreads();
-        }
-        if (pe >= n)
-            break;
-        // (2) stage L21 (rows [pe, n) of the panel) as FP64
-        for (int i = pe + tid; i < n; i += BT)
-#pragma unroll
-            for (int k = 0; k < BR; ++k)
-                if (k < jb)
-                    s_u[(i - pe) * BR + k] = pd(A[i + (size_t)(kb + k) * lda]);
-        __syncthreads();
-        // (3) the lower trailing block: a_ic += (-l_ck)*l_ik, k = kb .. pe-1 in order
-        for (int i = pe + tid; i < n; i += BT) {
-            double l[BR];
-#pragma unroll
-            for (int k = 0; k < BR; ++k)
-                l[k] = k < jb ? s_u[(i - pe) * BR + k] : 0.0;
-            for (int c = pe; c <= i; ++c) {
-                uint32_t *pa = A + i + (size_t)c * lda;
-                double a = pd(*pa);
-#pragma unroll
-                for (int k = 0; k < BR; ++k)
-                    if (k < jb)
-                        a = mac(a, -s_u[(c - pe) * BR + k], l[k]);
-                *pa = p32_from_double_exact(a);
-            }
-        }
-        __syncthreads();
-    }
-    return 0;
-}
-
 // Rgetrf (as unblocked right-looking LU) + Rgetrs('N') for one problem.
 __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key, int *s_idx, uint32_t *s_row)
 {
@@ -321,10 +93,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
     int info = 0;
     __shared__ uint32_t s_piv, s_recip;
     __shared__ int s_mode;
-    const bool blocked = factor && n <= BLOCKED_MAX_N;
-    if (blocked)
-        info = lu_factor_blocked(pr, s_key, s_idx, reinterpret_cast<double *>(s_row));
-    for (int k = 0; k < (factor && !blocked ? n : 0); ++k) {
+    for (int k = 0; k < (factor ? n : 0); ++k) {
         uint32_t *ck = A + (size_t)k * lda;
         const int p = iramax_block(ck, k, n, s_key, s_idx);
         const uint32_t piv = ck[p];
@@ -443,10 +212,7 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
     __shared__ uint32_t s_recip;
     __shared__ int s_fail;
     int info = 0;
-    const bool blocked = factor && n <= BLOCKED_MAX_N;
-    if (blocked)
-        info = chol_factor_blocked(pr, reinterpret_cast<double *>(s_row));
-    for (int k = 0; k < (factor && !blocked ? n : 0); ++k) {
+    for (int k = 0; k < (factor ? n : 0); ++k) {
         uint32_t *ck = A + (size_t)k * lda;
         if (tid == 0) {
             uint32_t akk = ck[k];

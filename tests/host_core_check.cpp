@@ -315,135 +315,4 @@ int hc_scan_row_check(uint32_t c0, const uint32_t *qp, int n, int E, long *stats
     const double b = scan_row_emul(p32_to_double(c0), q.data(), n, E, &stats[0], &stats[1]);
     return p32_from_double(a) == p32_from_double(b);
 }
-
-// The batched kernel's blocked factorizations (batch.cu, lu_factor_blocked and
-// chol_factor_blocked) written out sequentially with panel width R: the same element
-// operations in the same per-element order; returns info.
-static double mac_h(double c, double t, double a) { return f64_posit_mac_checked(c, t, a); }
-static int iramax_h(const uint32_t *col, int k, int n)
-{
-    int32_t best = INT32_MIN;
-    int bidx = n;
-    for (int i = k; i < n; ++i) {
-        const int32_t key = (int32_t)pabs(col[i]);
-        if (bidx == n || key > best) {
-            best = key;
-            bidx = i;
-        }
-    }
-    return bidx;
-}
-int hc_lu_blocked(int n, uint32_t *A, int lda, int *ipiv, int R)
-{
-    int info = 0;
-    std::vector<double> su((size_t)n * R + 1);
-    for (int kb = 0; kb < n; kb += R) {
-        const int jb = std::min(R, n - kb), pe = kb + jb;
-        for (int k = kb; k < pe; ++k) {
-            uint32_t *ck = A + (size_t)k * lda;
-            const int p = iramax_h(ck, k, n);
-            const uint32_t piv = ck[p];
-            ipiv[k] = p + 1;
-            int mode;
-            uint32_t recip = 0;
-            if (piv == 0) {
-                mode = 0;
-            } else if ((int32_t)pabs(piv) >= 1) {
-                mode = 1;
-                recip = pdiv(P32_ONE, piv);
-            } else {
-                mode = 2;
-            }
-            if (piv == 0 && info == 0)
-                info = k + 1;
-            if (piv != 0 && p != k)
-                for (int c = 0; c < n; ++c)
-                    std::swap(A[k + (size_t)c * lda], A[p + (size_t)c * lda]);
-            std::vector<double> u(R);
-            for (int c = 0; c < R; ++c)
-                u[c] = k + 1 + c < pe ? -p32_to_double(A[k + (size_t)(k + 1 + c) * lda]) : 0.0;
-            for (int i = k + 1; i < n; ++i) {
-                uint32_t l = ck[i];
-                if (mode == 1)
-                    l = pmul(recip, l);
-                else if (mode == 2)
-                    l = pdiv(l, piv);
-                ck[i] = l;
-                const double dl = p32_to_double(l);
-                for (int c = 0; c < R; ++c)
-                    if (k + 1 + c < pe) {
-                        uint32_t *pa = A + i + (size_t)(k + 1 + c) * lda;
-                        *pa = p32_from_double_exact(mac_h(p32_to_double(*pa), u[c], dl));
-                    }
-            }
-        }
-        if (pe >= n)
-            break;
-        for (int c = pe; c < n; ++c) {
-            uint32_t *ac = A + (size_t)c * lda;
-            std::vector<double> u(R);
-            for (int r = 0; r < jb; ++r) {
-                double v = p32_to_double(ac[kb + r]);
-                for (int k = 0; k < r; ++k)
-                    v = mac_h(v, -u[k], p32_to_double(A[kb + r + (size_t)(kb + k) * lda]));
-                u[r] = v;
-                ac[kb + r] = p32_from_double_exact(v);
-                su[(size_t)(c - pe) * R + r] = -v;
-            }
-        }
-        for (int i = pe; i < n; ++i) {
-            std::vector<double> l(R);
-            for (int k = 0; k < jb; ++k)
-                l[k] = p32_to_double(A[i + (size_t)(kb + k) * lda]);
-            for (int c = 0; c < n - pe; ++c) {
-                uint32_t *pa = A + i + (size_t)(pe + c) * lda;
-                double a = p32_to_double(*pa);
-                for (int k = 0; k < jb; ++k)
-                    a = mac_h(a, su[(size_t)c * R + k], l[k]);
-                *pa = p32_from_double_exact(a);
-            }
-        }
-    }
-    return info;
-}
-int hc_chol_blocked(int n, uint32_t *A, int lda, int R)
-{
-    std::vector<double> su((size_t)n * R + 1);
-    for (int kb = 0; kb < n; kb += R) {
-        const int jb = std::min(R, n - kb), pe = kb + jb;
-        for (int k = kb; k < pe; ++k) {
-            uint32_t *ck = A + (size_t)k * lda;
-            const uint32_t akk = ck[k];
-            if ((int32_t)akk <= 0)
-                return k + 1;
-            const uint32_t lkk = psqrt(akk);
-            ck[k] = lkk;
-            const uint32_t recip = pdiv(P32_ONE, lkk);
-            for (int i = k + 1; i < n; ++i)
-                ck[i] = pmul(recip, ck[i]);
-            for (int i = k + 1; i < n; ++i) {
-                const double li = p32_to_double(ck[i]);
-                for (int c = k + 1; c < pe; ++c)
-                    if (i >= c) {
-                        uint32_t *pa = A + i + (size_t)c * lda;
-                        *pa = p32_from_double_exact(mac_h(p32_to_double(*pa), -p32_to_double(ck[c]), li));
-                    }
-            }
-        }
-        if (pe >= n)
-            break;
-        for (int i = pe; i < n; ++i)
-            for (int k = 0; k < jb; ++k)
-                su[(size_t)(i - pe) * R + k] = p32_to_double(A[i + (size_t)(kb + k) * lda]);
-        for (int i = pe; i < n; ++i)
-            for (int c = pe; c <= i; ++c) {
-                uint32_t *pa = A + i + (size_t)c * lda;
-                double a = p32_to_double(*pa);
-                for (int k = 0; k < jb; ++k)
-                    a = mac_h(a, -su[(size_t)(c - pe) * R + k], su[(size_t)(i - pe) * R + k]);
-                *pa = p32_from_double_exact(a);
-            }
-    }
-    return 0;
-}
 }

@@ -37,8 +37,6 @@ def hc(tmp_path_factory):
     lib.hc_scan_row_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int, ctypes.c_int, I64]
     lib.hc_from_double_exact_mismatch.argtypes = [U32, ctypes.c_long]
     lib.hc_from_double_exact_mismatch.restype = ctypes.c_long
-    lib.hc_lu_blocked.argtypes = [ctypes.c_int, U32, ctypes.c_int, I32, ctypes.c_int]
-    lib.hc_chol_blocked.argtypes = [ctypes.c_int, U32, ctypes.c_int, ctypes.c_int]
     lib.hc_chain_reg_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.argtypes = [ctypes.c_uint32, U32, ctypes.c_int]
     lib.hc_chain_add.restype = ctypes.c_uint32
@@ -352,33 +350,3 @@ def test_exact_encode_round_trips_every_pattern_class(hc):
                         np.array([0, 1, 0x7FFFFFFF, 0x80000000, 0x80000001, 0xFFFFFFFF, 0x40000000], np.uint32)])
     assert hc.hc_from_double_exact_mismatch(np.ascontiguousarray(u), u.size) == 0
 
-
-def test_blocked_batch_factorizations_match_oracle(hc):
-    """The batched kernel's blocked LU and Cholesky (panels of R columns, U12 solve,
-    trailing block walked per row, every element updated in ascending k through the FP64
-    step), written out sequentially, equal the oracle's Rgetrf / Rpotrf('L'): factors,
-    pivots and info, for R = 1..8, zeros in the matrix, and singular and indefinite cases."""
-    rng = np.random.default_rng(51)
-    for trial in range(40):
-        n = int(rng.integers(1, 100))
-        R = int(rng.choice([1, 2, 3, 4, 8]))
-        A = oracle.from_double(rng.uniform(-1, 1, n * n))
-        if trial % 4 == 0:
-            A[::5] = 0
-        if trial % 7 == 0 and n > 3:
-            A[2 * n:3 * n] = 0  # a zero column: info > 0
-        g, o = A.copy(), A.copy()
-        gp, op = np.zeros(n, np.int32), np.zeros(n, np.int32)
-        assert hc.hc_lu_blocked(n, g, n, gp, R) == oracle.orc.orc_rgetrf(n, n, o, n, op, 64)
-        assert np.array_equal(g, o) and np.array_equal(gp, op), (n, R)
-        M = rng.uniform(-1, 1, (n, n))
-        S = M @ M.T / n + np.eye(n)
-        if trial % 6 == 0 and n > 4:
-            S[3, 3] = -1.0  # not positive definite at k = 3
-        S = oracle.from_double(S.reshape(-1, order="F"))
-        g, o = S.copy(), S.copy()
-        info = oracle.orc.orc_rpotrf(b"L", n, o, n, 64)
-        assert hc.hc_chol_blocked(n, g, n, R) == info, (n, R)
-        if info == 0:  # a stopped Cholesky leaves the rest of A unspecified (only info is defined)
-            lower = np.tril(np.ones((n, n), bool)).reshape(-1, order="F")
-            assert np.array_equal(g[lower], o[lower]), (n, R)
