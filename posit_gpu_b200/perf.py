@@ -16,16 +16,16 @@ SM_MAX_MHZ = 1965.0
 
 # Warp instructions issued by gemm_main_kernel per posit multiply-add:
 # smsp__inst_executed.sum / (m*n*k) for one NN launch at m = n = k = 4096
-# (57,500,845,547 / 68,719,476,736 = 0.8367, i.e. 26.78 thread instructions).  Of
+# (57,507,661,291 / 68,719,476,736 = 0.8368, i.e. 26.78 thread instructions).  Of
 # those, 11 per multiply-add run on the FP64 pipe (DMUL, DFMA, 7 DADD, 2 DSETP): FP64 pipe
-# 57.7 %, ALU pipe 44.2 %, issue 70.5 % busy in the same capture.
-WARP_INST_PER_MAD = 0.8367
+# 58.1 %, ALU pipe 44.5 %, issue 71.1 % busy in the same capture.
+WARP_INST_PER_MAD = 0.8368
 FP64_WARP_INST_PER_MAD = 11 / 32
 INST_SOURCE = ("ncu --set full, gemm_main_kernel<false,false>, NN 4096^3 U[-1,1] "
                "(profiles/gemm_main_kernel_nn_4096.md)")
 # DRAM bytes (read + write) per posit multiply-add of the same launch:
-# (7,250,573,000 + 73,805,824) / 68,719,476,736.
-MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1066
+# (7,385,502,000 + 71,760,128) / 68,719,476,736.
+MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1085
 
 
 def issue_peak_warp_inst_per_s(sm_mhz):
