@@ -6,14 +6,17 @@
 // operand alignment and its sticky-bit window, and correctly rounded division and
 // square root (no in-tree reference source exists for those two).
 //
-// Two layers:
+// Three layers:
 //   * pattern-level exact operations (padd, pmul, psub, pdiv, psqrt) -- decode with
-//     count-leading-zeros instead of the reference's bit-by-bit regime walk;
-//   * the decoded domain used by the GEMM inner loop: a value is held as
-//     (scale, significand, sign) with the significand's hidden bit at bit 30, so a
-//     multiply-add never re-decodes a bit pattern.  Zero and NaR are encoded as
-//     scales far outside the posit range (-1024 and 4096), which makes them fall out
-//     of the fast path's range test; the caller then redoes that step exactly.
+//     count-leading-zeros instead of the reference's bit-by-bit regime walk; the exact
+//     path of the two fast forms below;
+//   * the FP64 form (end of this file): posit values held in FP64, one multiply-add as a
+//     few FP64 operations that round onto the posit grid -- the GEMM, the column
+//     solves and the batched factorizations;
+//   * the decoded integer form: a value held as (scale, significand, sign) with the
+//     significand's hidden bit at bit 30 -- the one-thread triangular-solve chain
+//     (trsm_chain.cuh).  Zero is a scale far below the posit range, NaR stays outside
+//     (the callers carry it as a flag).
 #pragma once
 #include <stdint.h>
 #include <string.h>
@@ -345,14 +348,14 @@ PG_HD uint32_t pneg(uint32_t a) { return 0u - a; }
 PG_HD uint32_t pabs(uint32_t a) { return ((int32_t)a < 0) ? 0u - a : a; }
 
 // ----------------------------------------------------------------------------
-// Decoded-domain operations for the GEMM inner loop
+// Decoded integer form (the one-thread chain of trsm_chain.cuh)
 // ----------------------------------------------------------------------------
 //
-// The inner loop is integer code bound by the ALU pipe, so it is written to put as
-// much of its work as possible on the (otherwise idle) integer multiply-add pipe:
+// Integer code written to put as much of its work as possible on the integer
+// multiply-add pipe:
 //   * every quantity that depends only on a result's scale (regime run length, the
-//     multipliers that shift by it, whether the fast path is exact there) comes from a
-//     table indexed by that scale (one 16-byte shared-memory load);
+//     multipliers that shift by it, whether the fast path is exact there) comes from
+//     regime_entry, computed from that scale;
 //   * right shifts by n are multiplies by 2^(32-n) keeping the high word, and a 64-bit
 //     funnel shift is two multiply-adds;
 //   * round-to-nearest-even at bit 32 is one 64-bit add of 0x7FFFFFFF + lsb.
@@ -394,23 +397,20 @@ PG_HD uint32_t regime_run(int32_t s)
 
 PG_HD bool in_fast_range(int32_t s) { return (uint32_t)(s - FAST_LO) <= (uint32_t)(FAST_HI - FAST_LO); }
 
-// Decoded zero inside the GEMM kernels.  Any product with a zero operand then has a
-// scale <= ZERO_SCALE + 121 < ZERO_REGION, below every nonzero product (>= -241) and
+// Decoded zero.  Any product with a zero operand then has a
+// scale <= DECODED_ZERO_SCALE + 121 < ZERO_REGION, below every nonzero product (>= -241) and
 // every nonzero sum (>= -270), and its significand is 0.
-constexpr int32_t GEMM_ZERO_SCALE = -512;
+constexpr int32_t DECODED_ZERO_SCALE = -512;
 constexpr int32_t ZERO_REGION = -300;
 
-// Regime table: one entry per result scale s in [RT_MIN, RT_MAX].
-struct alignas(16) RegimeEntry {
+// Per result scale s: the rounding parameters of the decoded integer form (regime_entry).
+struct RegimeEntry {
     uint32_t r0;  // 2^(32-run): umulhi by it shifts right by run
     uint32_t nr1; // -(2^(31-run)); r0 + carry*nr1 = 2^(32-run-carry).  Bit 30 set
                   // means "a zero significand here is a failure" (clear in the zero region)
     uint32_t g;   // 2^(run+2): moves the kept bits back to a hidden bit at 30
     uint32_t w;   // 2^(29-run) (window multiplier for a hidden bit at 63), bit 30 = fail
 };
-constexpr int32_t RT_MIN = 2 * GEMM_ZERO_SCALE - 40;
-constexpr int32_t RT_MAX = 248;
-constexpr int32_t RT_N = RT_MAX - RT_MIN + 1;
 
 PG_HD RegimeEntry regime_entry(int32_t s)
 {
@@ -427,13 +427,8 @@ PG_HD RegimeEntry regime_entry(int32_t s)
     return e;
 }
 
-// Regime entry from the shared-memory table (throughput: the GEMM inner loops) or by
-// arithmetic (latency: one thread's chain of dependent additions, where a table load
-// would sit on the dependent path).
-struct TableEntry {
-    const RegimeEntry *tbl;
-    PG_HD_MEMBER RegimeEntry operator()(int32_t s) const { return tbl[s]; }
-};
+// Regime entry by arithmetic: one thread's chain of dependent additions, where a table
+// load would sit on the dependent path.
 struct ComputedEntry {
     PG_HD_MEMBER RegimeEntry operator()(int32_t s) const { return regime_entry(s); }
 };
@@ -457,11 +452,6 @@ PG_HD void dmul_core(const dp32 &t, const dp32 &a, EntryOf entry_of, dp32 &r, ui
     r.s = s;
     r.x = t.x ^ a.x;
     bad = e.w | (~r.g & e.nr1);
-}
-
-PG_HD void dmul_fast(const dp32 &t, const dp32 &a, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
-{
-    dmul_core(t, a, TableEntry{tbl}, r, bad);
 }
 
 // c + p rounded to posit32 (kernel_entry.cl:370-397), both decoded.  Fails (bit 30 of
@@ -506,34 +496,29 @@ PG_HD void dadd_core(const dp32 &c, const dp32 &p, EntryOf entry_of, dp32 &r, ui
     bad = e.w | (~r.g & e.nr1);
 }
 
-PG_HD void dadd_fast(const dp32 &c, const dp32 &p, const RegimeEntry *tbl, dp32 &r, uint32_t &bad)
-{
-    dadd_core(c, p, TableEntry{tbl}, r, bad);
-}
-
-// Exact decoded operations (through patterns): the slow path.  Decoded zeros of the
-// GEMM kernels (significand 0) encode to the zero pattern.
+// Exact decoded operations (through patterns): the slow path.  Decoded zeros
+// (significand 0) encode to the zero pattern.
 PG_HD_NOINLINE dp32 dmac_exact(dp32 c, dp32 t, dp32 a)
 {
     dp32 r = decode(padd(encode(c), pmul(encode(t), encode(a))));
     if (r.g == 0)
-        r.s = GEMM_ZERO_SCALE;
+        r.s = DECODED_ZERO_SCALE;
     return r;
 }
 
-// Decode for the GEMM kernels: zero gets GEMM_ZERO_SCALE; NaR is the caller's business.
-PG_HD dp32 decode_gemm(uint32_t u)
+// Decode with zero at DECODED_ZERO_SCALE; NaR is the caller's business.
+PG_HD dp32 decode_dz(uint32_t u)
 {
     dp32 d = decode(u);
     if (u == 0)
-        d.s = GEMM_ZERO_SCALE;
+        d.s = DECODED_ZERO_SCALE;
     return d;
 }
 
-// decode_gemm without branches (selects only), for a thread's dependent chain, where a
+// decode_dz without branches (selects only), for a thread's dependent chain, where a
 // branch would stop the next step's independent work from overlapping the current one.
 // u must not be NaR.
-PG_HD dp32 decode_gemm_bf(uint32_t u)
+PG_HD dp32 decode_dz_bf(uint32_t u)
 {
     const uint32_t x = u >> 31;
     const uint32_t v = x ? 0u - u : u;
@@ -543,21 +528,9 @@ PG_HD dp32 decode_gemm_bf(uint32_t u)
     const int32_t k = ones ? (int32_t)run - 1 : -(int32_t)run;
     const uint32_t rest = shl32(v, run + 2); // exponent at 31..30, fraction below
     dp32 r;
-    r.s = u == 0 ? GEMM_ZERO_SCALE : 4 * k + (int32_t)(rest >> 30);
+    r.s = u == 0 ? DECODED_ZERO_SCALE : 4 * k + (int32_t)(rest >> 30);
     r.g = u == 0 ? 0u : (P32_ONE | (rest & 0x3FFFFFFFu));
     r.x = x;
-    return r;
-}
-
-// c + t*a with both roundings; never fails.  tbl points at the entry for scale 0.
-PG_HD dp32 dmac(const dp32 &c, const dp32 &t, const dp32 &a, const RegimeEntry *tbl)
-{
-    dp32 p, r;
-    uint32_t bm, ba;
-    dmul_fast(t, a, tbl, p, bm);
-    dadd_fast(c, p, tbl, r, ba);
-    if ((bm | ba) & 0x40000000u)
-        r = dmac_exact(c, t, a);
     return r;
 }
 

@@ -22,8 +22,8 @@ namespace pg {
 
 constexpr int CHAIN_BLOCK = 8;
 
-PG_HD dp32 chain_neg_b(uint32_t bk) { return decode_gemm_bf(bk == P32_NAR ? 0u : 0u - bk); }
-PG_HD dp32 chain_a(uint32_t l) { return decode_gemm_bf(l == P32_NAR ? 0u : l); }
+PG_HD dp32 chain_neg_b(uint32_t bk) { return decode_dz_bf(bk == P32_NAR ? 0u : 0u - bk); }
+PG_HD dp32 chain_a(uint32_t l) { return decode_dz_bf(l == P32_NAR ? 0u : l); }
 
 // b (this thread's right-hand side, m entries; shared or global memory) is overwritten
 // with L^-T b.  L is read-only.  Host and device (the host build is what the CPU tests run).
@@ -34,7 +34,7 @@ PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, in
         const uint32_t *li = L + (size_t)i * ldl; // column i of L: a_ki for k > i
         const uint32_t bi = b[i];                 // alpha*b with alpha == 1
         uint32_t nar = bi == P32_NAR;
-        dp32 c = decode_gemm(nar ? 0u : bi);
+        dp32 c = decode_dz(nar ? 0u : bi);
         int k = i + 1;
         if (k + U <= m) {
             uint32_t lv[U], bv[U];

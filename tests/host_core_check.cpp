@@ -6,52 +6,40 @@
 #include <algorithm>
 #include <vector>
 using namespace pg;
-static RegimeEntry g_table[RT_N];
-static const RegimeEntry *table()
-{
-    static bool built = false;
-    if (!built) {
-        for (int i = 0; i < RT_N; i++)
-            g_table[i] = regime_entry(RT_MIN + i);
-        built = true;
-    }
-    return g_table - RT_MIN;
-}
 extern "C" {
 void hc_pmul_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = pmul(a[i], b[i]); }
 void hc_padd_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = padd(a[i], b[i]); }
 void hc_pdiv_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = pdiv(a[i], b[i]); }
 void hc_psqrt_n(const uint32_t *a, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = psqrt(a[i]); }
 void hc_from_double_n(const double *x, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = p32_from_double(x[i]); }
-// c + t*a through the decoded fast path (with its exact fallback); counts fast-path steps
+// c + t*a through the decoded integer form (computed regime entries, exact fallback), as
+// llt_chain runs it; counts the steps the fast path did alone
 long hc_dmac_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, uint32_t *o, long n)
 {
-    // NaR operands are handled outside the decoded domain by the GEMM kernels (flags);
-    // here they take the exact path directly.
-    const RegimeEntry *tb = table();
+    // NaR operands are handled outside the decoded domain (flags); here they take the
+    // exact path directly.
     long fast = 0;
     for (long i = 0; i < n; i++) {
         if (c[i] == P32_NAR || t[i] == P32_NAR || a[i] == P32_NAR) {
             o[i] = padd(c[i], pmul(t[i], a[i]));
             continue;
         }
-        dp32 dc = decode_gemm(c[i]), dt = decode_gemm(t[i]), da = decode_gemm(a[i]), p, r;
+        dp32 dc = decode_dz(c[i]), dt = decode_dz(t[i]), da = decode_dz(a[i]), p, r;
         uint32_t bm, ba;
-        dmul_fast(dt, da, tb, p, bm);
-        dadd_fast(dc, p, tb, r, ba);
+        dmul_core(dt, da, ComputedEntry{}, p, bm);
+        dadd_core(dc, p, ComputedEntry{}, r, ba);
         fast += !((bm | ba) & 0x40000000u);
-        o[i] = encode(dmac(dc, dt, da, tb));
+        o[i] = encode(dmac_chain(dc, dt, da));
     }
     return fast;
 }
 // a chain c <- c + t_l*a_l kept in the decoded domain for len steps
 void hc_chain(const uint32_t *c0, const uint32_t *t, const uint32_t *a, uint32_t *o, long nchains, long len)
 {
-    const RegimeEntry *tb = table();
     for (long j = 0; j < nchains; j++) {
-        dp32 c = decode_gemm(c0[j]);
+        dp32 c = decode_dz(c0[j]);
         for (long l = 0; l < len; l++)
-            c = dmac(c, decode_gemm(t[j * len + l]), decode_gemm(a[j * len + l]), tb);
+            c = dmac_chain(c, decode_dz(t[j * len + l]), decode_dz(a[j * len + l]));
         o[j] = encode(c);
     }
 }
@@ -63,19 +51,19 @@ void hc_dmac_chain_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, ui
             o[i] = P32_NAR;
             continue;
         }
-        o[i] = encode(dmac_chain(decode_gemm(c[i]), decode_gemm(t[i]), decode_gemm(a[i])));
+        o[i] = encode(dmac_chain(decode_dz(c[i]), decode_dz(t[i]), decode_dz(a[i])));
     }
 }
 // one right-hand side of the L^T solve: trsm_chain.cuh's llt_chain, built for the host
 void hc_llt_solve(const uint32_t *L, long ld, uint32_t *b, int m) { llt_chain(L, (size_t)ld, b, m, false); }
-// decode_gemm_bf against decode_gemm on n patterns (NaR skipped); returns mismatches
+// decode_dz_bf against decode_dz on n patterns (NaR skipped); returns mismatches
 long hc_decode_bf_mismatch(const uint32_t *u, long n)
 {
     long bad = 0;
     for (long i = 0; i < n; i++) {
         if (u[i] == P32_NAR)
             continue;
-        const dp32 a = decode_gemm(u[i]), b = decode_gemm_bf(u[i]);
+        const dp32 a = decode_dz(u[i]), b = decode_dz_bf(u[i]);
         bad += (a.s != b.s) | (a.g != b.g) | (a.x != b.x);
     }
     return bad;
