@@ -2,9 +2,10 @@
 // launch fed by a device work queue of output tiles.
 //
 // The queue holds (problem, tile row, tile column, tile shape) items sorted by
-// decreasing k.  A CTA takes the next item, loads and decodes its operands straight from
-// the problem's matrices (transposes and alpha*B for the NN/NT order handled during the
-// load), and runs the same k-step routine as the single-GEMM kernel (gemm_tile.cuh), so
+// decreasing k.  A CTA takes the next item, loads its operands straight from the
+// problem's matrices into FP64 tiles (transposes and alpha*B for the NN/NT order handled
+// during the load), and runs the same k-step routine as the single-GEMM kernel
+// (gemm_tile.cuh, tile_steps_f64), so
 // every C is bit-identical to posit_rgemm_dev's, i.e. to the CPU Rgemm.  Three tile
 // shapes (64x32, 32x32, 32x64 outputs per CTA) cover small and skinny problems; which one
 // a problem uses comes from a table indexed by its (m, n) size bucket, produced by the

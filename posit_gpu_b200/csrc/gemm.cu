@@ -11,16 +11,18 @@
 // epilogue.  So one main kernel serves all four transpose cases:
 //
 //  1. decode pre-pass: op(A) and op(B) (times alpha for NN/NT, rounded exactly as the
-//     reference rounds alpha*b_lj) are decoded ONCE per element into
-//     (scale, significand|sign) pairs, stored tile-contiguously in a workspace:
-//     A as [m-tile][k-tile][l][i], B as [n-tile][k-tile][l][j].  Transposition is
-//     absorbed here, so the main kernel never sees lda/ldb.
-//  2. main kernel: one CTA per 64x64 tile of C, 256 threads, 4x4 outputs per thread
-//     held in decoded form across the whole k loop.  Each 16-deep k tile of A and B
-//     (8 KB each) is brought into shared memory by the bulk-copy (TMA) engine
-//     (cp.async.bulk + mbarrier transaction counts, 3 stages).  The inner step is
-//     integer-only and branch-free; the rare step that leaves the fast range (long
-//     regimes, zero or NaR operands, exact cancellation) is redone exactly afterwards.
+//     reference rounds alpha*b_lj) are converted ONCE per element to FP64 (posit32
+//     values are exact there), stored tile-contiguously in a workspace: A as
+//     [m-tile][k-tile][l][i], B as [n-tile][k-tile][l][j], plus a NaR flag per row and
+//     column.  Transposition is absorbed here, so the main kernel never sees lda/ldb.
+//  2. main kernel: one CTA per 64x32 tile of C, 256 threads, 4x2 outputs per thread held
+//     in FP64 across the whole k loop, 4 CTAs per SM.  Each 16-deep k tile of A and B
+//     (8 KB + 4 KB) is brought into shared memory by the bulk-copy (TMA) engine
+//     (cp.async.bulk + mbarrier transaction counts, 3 stages, every wait bounded).  The
+//     inner step is the FP64 form of p32_mul + p32_add (posit32.cuh, f64_posit_mac) with
+//     the rounding constants in a shared-memory table, committed branch-free; the rare
+//     step it flags (an inexact FP64 sum, a result outside the fast window) is redone
+//     exactly, in order, right after its k step.
 #include "gemm.cuh"
 #include "gemm_tile.cuh"
 #include "posit32.cuh"

@@ -11,9 +11,11 @@
 // block size bit for bit (the zero-multiplier skips of Rtrsm/Rsyrk add zero and change
 // nothing unless a NaR is present), and the device code may block the work its own way:
 //
-//   panel (nb columns)   one kernel per column: pivot search + row interchange
-//                        (LU only, one CTA), then scale the column and apply the rank-1
-//                        update to the rest of the panel (all rows in parallel);
+//   panel (nb columns)   two kernels per column, ordered by the kernel boundary alone:
+//                        the pivot (LU: iRamax and the row interchange) or diagonal
+//                        (Cholesky: square root) step of one CTA, then the scaling of
+//                        the column and the rank-1 update of the rest of the panel over
+//                        all rows in parallel;
 //   U block row          Rtrsm("L","L","N","U") as one CTA per column;
 //   row interchanges     Rlaswp on the columns outside the panel;
 //   trailing update      the posit32 GEMM of gemm.cu (NN for LU; NT restricted to the

@@ -1,13 +1,18 @@
-// trsm_chain.cuh -- the transposed lower triangular solve of Rpotrs as one thread's chain.
+// trsm_chain.cuh -- the transposed lower triangular solve of Rpotrs: chains of dependent
+// posit additions.
 //
 // Rtrsm('L', 'L', 'T', 'N'), Rtrsm.cpp:175-186: for i = m-1 down to 0,
 //     t = b_i;  t = t - a_ki * b_k  for k = i+1 .. m-1 (ascending);  b_i = t / a_ii.
 // Each b_i's sum starts from the b_{i+1} just finished, so one right-hand side is a single
-// chain of m(m-1)/2 dependent multiply-subtracts with two roundings each.  A thread owns one
-// right-hand side and runs its whole chain with the accumulator held decoded; different
-// right-hand sides are different threads.
+// chain of m(m-1)/2 dependent multiply-subtracts with two roundings each.  Three forms:
+//   * llt_chain: one thread runs a right-hand side's whole chain with the accumulator
+//     held in the decoded integer form (the batched kernel; very long columns);
+//   * chain_add_run / chain_add_run_reg: one thread's chain of additions in FP64, the
+//     products computed elsewhere;
+//   * the scan form (below): a warp sums a row's additions as a parallel prefix of step
+//     maps on the posit grid (lapack.cu's transposed-solve kernel).
 //
-// Latency is everything here.  Only the addition depends on the previous step: loads,
+// For the one-thread chains latency is everything.  Only the addition depends on the previous step: loads,
 // decoding and the product of step k+1 can overlap the addition of step k, but not across
 // a branch (a GPU issues in order and does not run past an unresolved branch).  So the
 // steps run in blocks of CHAIN_BLOCK without a branch: the fast path's failure flags are
