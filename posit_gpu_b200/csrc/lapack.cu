@@ -88,22 +88,34 @@ __global__ void __launch_bounds__(1024) lu_pivot_kernel(uint32_t *__restrict__ P
             bidx = i;
         }
     }
-    s_key[tid] = best;
-    s_idx[tid] = bidx;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (tid < s) {
-            int32_t k2 = s_key[tid + s];
-            int i2 = s_idx[tid + s];
-            bool take = i2 >= 0 && (s_idx[tid] < 0 || k2 > s_key[tid] || (k2 == s_key[tid] && i2 < s_idx[tid]));
-            if (take) {
-                s_key[tid] = k2;
-                s_idx[tid] = i2;
+    // larger key wins, equal keys the smaller row; warp shuffles, then one warp over the
+    // warps' results (blockDim.x == 1024: 32 warps)
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int round = 0; round < 2; ++round) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const int32_t k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
+            const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
+            if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
+                best = k2;
+                bidx = i2;
             }
         }
-        __syncthreads();
+        if (round == 0) {
+            if (lane == 0) {
+                s_key[warp] = best;
+                s_idx[warp] = bidx;
+            }
+            __syncthreads();
+            best = s_key[lane];
+            bidx = s_idx[lane];
+        }
     }
-    const int p = s_idx[0];
+    if (tid == 0)
+        s_idx[32] = bidx;
+    __syncthreads();
+    const int p = s_idx[32];
     const uint32_t piv = col[p];
     if (tid == 0) {
         ipiv[row0 + k] = row0 + p + 1; // 1-based, global
@@ -149,13 +161,13 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
                                                                const PivotInfo *__restrict__ pinfo,
                                                                uint32_t *__restrict__ lcol)
 {
-    __shared__ uint32_t s_u[PANEL_CG]; // -u_kc for this block's columns
+    __shared__ double s_u[PANEL_CG]; // -u_kc for this block's columns, FP64
     if (*info < 0)
         return;
     const PivotInfo pi = *pinfo;
     const int c0 = k + 1 + blockIdx.y * PANEL_CG;
     if (threadIdx.x < PANEL_CG && c0 + (int)threadIdx.x < jb)
-        s_u[threadIdx.x] = pneg(P[k + (size_t)(c0 + threadIdx.x) * lda]); // row k after the interchange
+        s_u[threadIdx.x] = -p32_to_double(P[k + (size_t)(c0 + threadIdx.x) * lda]); // row k after the interchange
     __syncthreads();
     const int i = k + 1 + blockIdx.x * PANEL_ROWS + threadIdx.x;
     if (i >= M)
@@ -163,10 +175,11 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
     const uint32_t l = lu_scaled(P[i + (size_t)k * lda], pi);
     if (blockIdx.y == 0)
         lcol[i] = l;
+    const double dl = p32_to_double(l);
     const int cn = min(PANEL_CG, jb - c0);
-    for (int j = 0; j < cn; ++j) {
+    for (int j = 0; j < cn; ++j) { // a_ic + (-u_kc)*l_i in the FP64 step (posit32.cuh)
         uint32_t *pc = P + i + (size_t)(c0 + j) * lda;
-        *pc = padd(*pc, pmul(s_u[j], l));
+        *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_u[j], dl));
     }
 }
 
@@ -591,14 +604,14 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
                                                                  const CholSync *__restrict__ sync,
                                                                  uint32_t *__restrict__ lcol)
 {
-    __shared__ uint32_t s_l[PANEL_CG]; // -l_ck for this block's columns
+    __shared__ double s_l[PANEL_CG]; // -l_ck for this block's columns, FP64
     if (*info != 0)
         return;
     const uint32_t recip = sync->recip;
     const uint32_t *pk = P + (size_t)k * lda;
     const int c0 = k + 1 + blockIdx.y * PANEL_CG;
     if (threadIdx.x < PANEL_CG && c0 + (int)threadIdx.x < jb)
-        s_l[threadIdx.x] = pneg(pk[c0 + threadIdx.x]); // scaled by the diagonal step
+        s_l[threadIdx.x] = -p32_to_double(pk[c0 + threadIdx.x]); // scaled by the diagonal step
     __syncthreads();
     const int i = k + 1 + blockIdx.x * PANEL_ROWS + threadIdx.x;
     if (i >= M)
@@ -607,10 +620,11 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
     const uint32_t l = i >= jb ? pmul(recip, a) : a;
     if (blockIdx.y == 0 && i >= jb)
         lcol[i] = l;
+    const double dl = p32_to_double(l);
     const int cn = min(min(PANEL_CG, jb - c0), i - c0 + 1);
-    for (int j = 0; j < cn; ++j) {
+    for (int j = 0; j < cn; ++j) { // a_ic + (-l_ck)*l_i in the FP64 step (posit32.cuh)
         uint32_t *pc = P + i + (size_t)(c0 + j) * lda;
-        *pc = padd(*pc, pmul(s_l[j], l));
+        *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_l[j], dl));
     }
 }
 
