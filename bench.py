@@ -209,6 +209,24 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# multi-rank timing: every rank times its own replica; the job's time is the slowest
+# rank's, and the job's rate counts the work of all ranks
+# ---------------------------------------------------------------------------
+def max_over_ranks(x, dist, device):
+    """x, maximised over the ranks of the default process group (dist None: one rank)."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, work_per_step, steps, ms_max):
+    """Units per second of the whole job: world replicas, `steps` steps each, in ms_max."""
+    return world * work_per_step * steps / (ms_max / 1e3)
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def ours(args):
@@ -281,12 +299,9 @@ def ours(args):
     ms = e0.elapsed_time(e1)
     if pg.device_error(True):
         raise RuntimeError("device error flag raised during the timed region")
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, dev)
     ops_per_step = 2.0 * m * n * k
-    value = world * ops_per_step * args.steps / (ms_max / 1e3) / 1e9
+    value = whole_job_rate(world, ops_per_step, args.steps, ms_max) / 1e9
 
     # roofline of the main kernel: instruction issue (FP64 pipe the busiest pipe)
     mads = float(m) * n * k
@@ -348,10 +363,7 @@ def ours(args):
         for _ in range(esteps):
             pg.Rgemm(ta, tb, m, n, k, alpha, nA, lda, nB, ldb, beta, nC, m)
         e2e_s = time.perf_counter() - t0
-        te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_s = float(te.item())
+        e2e_s = max_over_ranks(e2e_s, dist, dev)
         line["e2e"] = {"value": round(world * ops_per_step * esteps / e2e_s / 1e9, 3), "unit": UNIT,
                        "h2d_bytes_per_step": 4 * (m * k + k * n + m * n), "d2h_bytes_per_step": 4 * m * n,
                        "steps": esteps, "timing": "host wall clock around the synchronous call"}
