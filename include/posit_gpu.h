@@ -64,8 +64,11 @@ int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alph
  * whose posit_rgemm_workspace_size exceeds that size return POSIT_E_NOALLOC_LIMIT (e.g.
  * 2048 x 2048 x 2032 fits, 2048^3 does not; an 8192 x 8192 x 256 trailing update needs
  * 34 MB and fits).
+ * Argument errors return the Rgemm info code first; calls that form no product (alpha
+ * == 0, k == 0, the quick returns) use no scratch and are never refused.
  * The first call on a device looks up the array's address; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * capture, and do not call it again after a cudaDeviceReset (the cached address is then
+ * stale).  All calls share the array: calls that overlap on the GPU race. */
 #define POSIT_NOALLOC_SCRATCH_BYTES (64u << 20)
 int posit_rgemm_dev_noalloc(char transa, char transb, int m, int n, int k, uint32_t alpha,
                             const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,

@@ -113,14 +113,22 @@ __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, double *As, d
     }
 }
 
-// alpha == 0 or k == 0 with beta != 1 (Rgemm.cpp:142-156): C <- 0 or beta*C on the tile
+// alpha == 0 or k == 0 with beta != 1, on the tile: C <- 0 or beta*C (alpha == 0,
+// Rgemm.cpp:142-156; NN/NT with k == 0, Rgemm.cpp:169-177).  TN/TT with k == 0 and
+// alpha != 0 form alpha*0 and combine it with beta*C (Rgemm.cpp:193-201): NaR when alpha
+// is NaR.
 __device__ void batch_scale_tile(const BatchGemmDesc &P, int mt, int nt, int bm, int bn)
 {
+    const bool dot = P.alpha != 0 && !P.nota;
+    const uint32_t t = pmul(P.alpha, 0u);
     for (int e = threadIdx.x; e < bm * bn; e += BG_THREADS) {
         const int row = mt * bm + e % bm, col = nt * bn + e / bm;
         if (row < P.m && col < P.n) {
             uint32_t *cp = P.C + (size_t)row + (size_t)col * P.ldc;
-            *cp = (P.beta == 0) ? 0u : pmul(P.beta, *cp);
+            if (dot)
+                *cp = (P.beta == 0) ? t : padd(t, pmul(P.beta, *cp));
+            else
+                *cp = (P.beta == 0) ? 0u : pmul(P.beta, *cp);
         }
     }
 }

@@ -33,8 +33,11 @@ int cuda_fail(cudaError_t e)
 bool same(char a, char b) { return toupper((unsigned char)a) == toupper((unsigned char)b); }
 int imax(int a, int b) { return a > b ? a : b; }
 
+} // namespace
+
+namespace pg {
 // Rgemm.cpp:90-128: argument checks in the reference's order.
-int check_args(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, bool &nota, bool &notb)
+int rgemm_check_args(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, bool &nota, bool &notb)
 {
     nota = same(ta, 'N');
     notb = same(tb, 'N');
@@ -57,6 +60,10 @@ int check_args(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc,
         return 13;
     return 0;
 }
+} // namespace pg
+
+namespace {
+using pg::rgemm_check_args;
 
 // Keep stream-ordered allocations cached in the device's default pool instead of
 // returning them to the driver at every synchronisation.
@@ -91,8 +98,10 @@ int rgemm_device(bool nota, bool notb, int m, int n, int k, uint32_t alpha, cons
     if (m == 0 || n == 0 || ((alpha == 0 || k == 0) && beta == pg::P32_ONE))
         return 0;
     if (alpha == 0 || k == 0) {
-        // k == 0 leaves beta*C (NN/NT scale C, TN/TT form alpha*0 + beta*C == beta*C)
-        PG_TRY(pg::scale_launch(m, n, beta, C, ldc, st));
+        // alpha == 0: C <- 0 or beta*C (Rgemm.cpp:142-156).  k == 0: NN/NT only scale C
+        // (Rgemm.cpp:169-177); TN/TT still form alpha*0 and combine it with beta*C
+        // (Rgemm.cpp:193-201), NaR when alpha is NaR.
+        PG_TRY(pg::scale_launch(m, n, alpha != 0 && !nota, alpha, beta, C, ldc, st));
         return 0;
     }
     size_t need = pg::gemm_workspace_bytes(m, n, k);
@@ -138,7 +147,7 @@ int posit_rgemm_dev(char transa, char transb, int m, int n, int k, uint32_t alph
                     size_t workspace_bytes, void *stream)
 {
     bool nota, notb;
-    int info = check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
+    int info = rgemm_check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
     if (info)
         return info;
     int r = ensure_init();
@@ -152,7 +161,7 @@ int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, c
                 const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc)
 {
     bool nota, notb;
-    int info = check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
+    int info = rgemm_check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
     if (info)
         return info;
     if (m == 0 || n == 0 || ((alpha == 0 || k == 0) && beta == pg::P32_ONE))

@@ -296,14 +296,23 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     }
 }
 
-__global__ void scale_kernel(int m, int n, uint32_t beta, uint32_t *__restrict__ C, size_t ldc)
+// C <- 0 or beta*C (alpha == 0, Rgemm.cpp:142-156; NN/NT with k == 0, Rgemm.cpp:169-177), or,
+// with `dot`, the dot-then-combine epilogue of an empty sum (TN/TT with k == 0,
+// Rgemm.cpp:193-201): t = alpha*0, then c = t (beta == 0) or t + beta*c.  alpha*0 is NaR
+// when alpha is NaR (p32_mul tests NaR before zero, kernel_entry.cl:414-421).
+__global__ void scale_kernel(int m, int n, bool dot, uint32_t alpha, uint32_t beta, uint32_t *__restrict__ C,
+                             size_t ldc)
 {
     size_t total = (size_t)m * n;
+    const uint32_t t = pmul(alpha, 0u);
     for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         size_t i = idx % m, j = idx / m;
         uint32_t *cp = C + i + j * ldc;
-        *cp = (beta == 0) ? 0u : pmul(beta, *cp); // Rgemm.cpp:142-156
+        if (dot)
+            *cp = (beta == 0) ? t : padd(t, pmul(beta, *cp));
+        else
+            *cp = (beta == 0) ? 0u : pmul(beta, *cp);
     }
 }
 
@@ -448,9 +457,10 @@ cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_
                                   stop);
 }
 
-cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream)
+cudaError_t scale_launch(int m, int n, bool dot, uint32_t alpha, uint32_t beta, uint32_t *C, int ldc,
+                         cudaStream_t stream)
 {
-    scale_kernel<<<grid_for((size_t)m * n, 256), 256, 0, stream>>>(m, n, beta, C, (size_t)ldc);
+    scale_kernel<<<grid_for((size_t)m * n, 256), 256, 0, stream>>>(m, n, dot, alpha, beta, C, (size_t)ldc);
     prof_count(1);
     return cudaGetLastError();
 }

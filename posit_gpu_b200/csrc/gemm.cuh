@@ -28,6 +28,10 @@ struct GemmPlan {
 };
 
 GemmPlan gemm_plan(int m, int n, int k);
+
+// The Rgemm argument checks (Rgemm.cpp:90-128) in the reference's order: 0, or the info
+// code of the first bad argument.  Sets nota/notb ('N' or 'n').
+int rgemm_check_args(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, bool &nota, bool &notb);
 size_t gemm_workspace_bytes(int m, int n, int k);
 
 // Decode op(A) and alpha*op(B) (or op(B) for the dot-then-combine order) into the
@@ -42,8 +46,11 @@ cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_
                               const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
                               uint32_t *C, int ldc, void *workspace, cudaStream_t stream, const int *stop);
 
-// C <- 0 or beta*C on the m x n submatrix (alpha == 0 or k == 0 with beta != 1).
-cudaError_t scale_launch(int m, int n, uint32_t beta, uint32_t *C, int ldc, cudaStream_t stream);
+// The calls that form no product (alpha == 0, or k == 0), on the m x n submatrix:
+// C <- 0 or beta*C; with `dot` (TN/TT and k == 0, alpha != 0) C <- alpha*0 or
+// alpha*0 + beta*C, which is NaR everywhere when alpha is NaR.
+cudaError_t scale_launch(int m, int n, bool dot, uint32_t alpha, uint32_t beta, uint32_t *C, int ldc,
+                         cudaStream_t stream);
 
 // Element-wise IEEE double <-> posit32 conversion on device buffers.
 cudaError_t convert_launch(bool to_posit, const void *in, void *out, size_t n, cudaStream_t stream);

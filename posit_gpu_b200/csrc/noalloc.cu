@@ -14,13 +14,19 @@
 // 64 MiB until the process exits.  Host code must not pass the symbol itself to a
 // kernel (on the host it names a shadow object, not device memory): the first call on
 // each device looks up the array's device address with cudaGetSymbolAddress, with that
-// device current, and caches it.  Make that first call before any stream capture.
+// device current, and caches it.  Make that first call before any stream capture.  A
+// cudaDeviceReset unloads the module and with it the array; the cached address is then
+// stale, so do not call this entry point again in a process that has reset the device.
 //
 // All calls on a device share the one array and it keeps whatever the last call left in
-// it.  Nothing in it has to start at zero: the decode pre-pass writes every scratch byte
-// the main kernel will read before that kernel runs.  Two calls whose work overlaps on
-// the GPU (e.g. issued on different streams without ordering) race on the array.
+// it.  Nothing in it has to start at zero from an earlier call: on every call the GEMM
+// launch clears the region of per-row and per-column NaR flags (a stream-ordered memset)
+// before the decode pre-pass sets the flags it finds, and the decode pre-pass writes every
+// byte of the operand-tile region before the main kernel reads it.  Two calls whose work
+// overlaps on the GPU (e.g. issued on different streams without ordering) race on the
+// array.
 #include "../../include/posit_gpu.h"
+#include "gemm.cuh"
 
 #include <cuda_runtime.h>
 #include <mutex>
@@ -60,14 +66,20 @@ extern "C" int posit_rgemm_dev_noalloc(char transa, char transb, int m, int n, i
                                        const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
                                        uint32_t *C, int ldc, void *stream)
 {
-    // Shapes whose decoded operands do not fit the static array are refused up front.
-    // (Bad arguments give a workspace size of 0 here and are reported by the checks of
-    // posit_rgemm_dev below, with the Rgemm info code.)
-    size_t need = posit_rgemm_workspace_size(transa, transb, m, n, k);
-    if (need > (size_t)POSIT_NOALLOC_SCRATCH_BYTES)
+    // The Rgemm argument checks come first, so a bad argument gets its info code whatever
+    // the shape.
+    bool nota, notb;
+    const int info = pg::rgemm_check_args(transa, transb, m, n, k, lda, ldb, ldc, nota, notb);
+    if (info)
+        return info;
+    // Only a call that runs the main GEMM (alpha != 0, k > 0, a non-empty C) uses scratch;
+    // the quick returns and the calls that only scale C need none and are never refused.
+    const bool uses_scratch = m > 0 && n > 0 && k > 0 && alpha != 0;
+    if (uses_scratch &&
+        posit_rgemm_workspace_size(transa, transb, m, n, k) > (size_t)POSIT_NOALLOC_SCRATCH_BYTES)
         return POSIT_E_NOALLOC_LIMIT;
     void *scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
+    const int rc = scratch_for_current_device(&scratch);
     if (rc)
         return rc;
     // With a caller-supplied workspace posit_rgemm_dev makes no allocation.

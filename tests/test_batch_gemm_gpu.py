@@ -77,3 +77,29 @@ def test_batch_gemm_rejects_bad_arguments(cuda_ok):
     t = torch.zeros(16, dtype=torch.int32, device="cuda")
     with pytest.raises(ValueError, match="parameter number  8"):
         pg.BatchGemmPlan([("N", "N", 4, 4, 4, ONE, t, 4, t, 4, 0, t, 4), ("N", "N", 4, 2, 2, ONE, t, 3, t, 2, 0, t, 4)])
+
+
+def test_batch_gemm_k0_every_alpha_beta(cuda_ok):
+    """k = 0 in the batched kernel: TN/TT form alpha*0 and combine it with beta*C
+    (Rgemm.cpp:190-203, 232-245), NaR for alpha = NaR; NN/NT only scale C."""
+    rng = np.random.default_rng(123)
+    probs = []
+    for ta in ("N", "T"):
+        for tb in ("N", "T"):
+            for alpha in (0, ONE, M1, oracle.p32(0.3), NAR):
+                for beta in (0, ONE, oracle.p32(0.5), NAR):
+                    m, n = int(rng.integers(1, 70)), int(rng.integers(1, 70))
+                    C = oracle.from_double(rng.uniform(-1, 1, m * n))
+                    C[0] = NAR
+                    z = np.zeros(max(1, m * n), np.uint32)
+                    probs.append((ta, tb, m, n, 0, alpha, z, max(1, m), z.copy(), max(1, n), beta, C, m))
+    outs = _run(probs)
+    for p, got in zip(probs, outs):
+        ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc = p
+        want = C.copy()
+        oracle.rgemm(ta, tb, m, n, k, al, A, lda, B, ldb, be, want, ldc)
+        if oracle.ref is not None:
+            w2 = C.copy()
+            oracle.ref.ref_rgemm(ta.encode(), tb.encode(), m, n, k, al, A, lda, B, ldb, be, w2, ldc)
+            assert np.array_equal(w2, want)
+        assert np.array_equal(got, want), (ta, tb, m, n, hex(al), hex(be))

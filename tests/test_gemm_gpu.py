@@ -111,3 +111,48 @@ def test_only_submatrix_touched(cuda_ok):
     for j in range(n):
         mask[j * ldc:j * ldc + m] = True
     assert np.array_equal(Cg[~mask], C[~mask])
+
+
+K0_ALPHAS = [0, ONE, M1, oracle.p32(0.3), NAR]
+K0_BETAS = [0, ONE, oracle.p32(0.5), NAR]
+
+
+def _k0_want(ta, tb, m, n, alpha, beta, C):
+    """k = 0 through the restatement and, where built, the reference's own Rgemm: for
+    TN/TT it still forms alpha*0 and combines it with beta*C (Rgemm.cpp:190-203,
+    232-245), so alpha = NaR gives NaR."""
+    z = np.zeros(max(1, m * n), np.uint32)
+    want = C.copy()
+    assert oracle.rgemm(ta, tb, m, n, 0, alpha, z, max(1, m), z, max(1, n), beta, want, m) == 0
+    if oracle.ref is not None:
+        w2 = C.copy()
+        oracle.ref.ref_rgemm(ta.encode(), tb.encode(), m, n, 0, alpha, z, max(1, m), z, max(1, n), beta, w2, m)
+        assert np.array_equal(w2, want), "restatement and reference disagree at k = 0"
+    return want
+
+
+@pytest.mark.parametrize("ta,tb", TRANS)
+def test_k0_every_alpha_beta(cuda_ok, ta, tb):
+    """k = 0, every (alpha, beta) of the special set, on the host, device and no-alloc
+    entry points."""
+    import torch
+
+    import posit_gpu_b200 as pg
+    rng = np.random.default_rng(5)
+    m, n = 19, 13
+    z = np.zeros(max(1, m * n), np.uint32)
+    C = pd.uniform(rng, (m * n,))
+    C[3], C[7] = NAR, 0
+    for alpha in K0_ALPHAS:
+        for beta in K0_BETAS:
+            want = _k0_want(ta, tb, m, n, alpha, beta, C)
+            Cg = C.copy()
+            pg.Rgemm(ta, tb, m, n, 0, alpha, z, max(1, m), z, max(1, n), beta, Cg, m)
+            assert np.array_equal(Cg, want), ("host", hex(alpha), hex(beta))
+            dz = torch.zeros(max(1, m * n), dtype=torch.int32, device="cuda")
+            for fn in (pg.Rgemm_dev, pg.Rgemm_dev_noalloc):
+                dC = torch.from_numpy(C.view(np.int32).copy()).cuda()
+                fn(ta, tb, m, n, 0, alpha, dz, max(1, m), dz, max(1, n), beta, dC, m)
+                torch.cuda.synchronize()
+                got = dC.cpu().numpy().view(np.uint32)
+                assert np.array_equal(got, want), (fn.__name__, hex(alpha), hex(beta))
