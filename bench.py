@@ -55,6 +55,7 @@ def parse():
                     help="gemm: the LU trailing-update shape m = n = N-b, k = b (b = this value, N = --n)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true", help="gemm: skip the sampled bit-exact check")
     ap.add_argument("--workload", default="gemm", choices=["gemm", "lu", "cholesky", "batch", "serve"],
                     help="gemm (default, the headline), lu / cholesky (device-resident "
                          "factorization + solve, FP64 errors), batch (batched vs per-call)")
@@ -251,19 +252,9 @@ def ours(args):
     pg.init()
     m, n, k = shape(args)
     ta, tb = args.trans[0], args.trans[1]
-    lda = m if ta in "nN" else k
-    ldb = k if tb in "nN" else n
     alpha, beta = pg.P32_MINUS_ONE, pg.P32_ONE
-    g = torch.Generator(device=dev)
-    g.manual_seed(1234 + rank)
-
-    def rand_posit(numel):
-        x = torch.rand(numel, dtype=torch.float64, device=dev, generator=g) * 2.0 - 1.0
-        return pg.from_double_dev(x)
-
-    A = rand_posit(m * k)
-    B = rand_posit(k * n)
-    C = rand_posit(m * n)
+    from posit_gpu_b200 import workloads
+    A, lda, B, ldb, C, _ = workloads.gemm_operands(m, n, k, ta, tb, seed=workloads.GEMM_SEED + rank, device=dev)
     ws = torch.empty(pg.workspace_size(ta, tb, m, n, k), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -309,14 +300,16 @@ def ours(args):
     sm_mhz = clocks.get("sm_mhz") or perf.SM_MAX_MHZ
     peak = perf.issue_peak_warp_inst_per_s(sm_mhz)
     achieved = None
-    if perf.WARP_INST_PER_MAD and main_avg_s > 0:
+    current = perf.inst_count_current()
+    if perf.WARP_INST_PER_MAD and main_avg_s > 0 and current:
         achieved = perf.WARP_INST_PER_MAD * mads / main_avg_s
     fp64_frac = (perf.FP64_WARP_INST_PER_MAD * mads / main_avg_s / perf.fp64_pipe_peak_warp_inst_per_s(sm_mhz)
                  if main_avg_s > 0 else None)
     roofline = {"bound": "issue", "achieved": achieved and round(achieved / 1e12, 4),
                 "peak": round(peak / 1e12, 4), "unit": "T warp-inst/s",
                 "frac": achieved and round(achieved / peak, 4),
-                "traffic": perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD and perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD * mads,
+                "traffic": (perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD * mads
+                            if perf.MAIN_KERNEL_DRAM_BYTES_PER_MAD and not args.trailing else None),
                 "kernel": "gemm_main_kernel<false,false>" if ta in "nN" else "gemm_main_kernel<true,false>",
                 "main_kernel_ms": round(main_avg_s * 1e3, 3),
                 "posit_gop_s_main_kernel": round(2 * mads / main_avg_s / 1e9, 2) if main_avg_s > 0 else None,
@@ -324,7 +317,14 @@ def ours(args):
                 "fp64_pipe_frac": fp64_frac and round(fp64_frac, 4),
                 "peak_basis": f"148 SMs x 4 SMSP x 1 warp-inst/clk at {sm_mhz:.0f} MHz (sampled median); "
                               "MEASURED_PEAKS.json has no issue or FP64 figure",
-                "inst_source": perf.INST_SOURCE}
+                "inst_source": perf.INST_SOURCE,
+                "inst_source_stale": not current,
+                "kernel_source_sha256": perf.kernel_source_digest()}
+    if not current:
+        roofline["fp64_pipe_frac"] = None
+    if args.trailing:  # measured per shape, never scaled from the cube
+        roofline["traffic"] = perf.trailing_traffic(k)
+        roofline["traffic_source"] = perf.TRAILING_TRAFFIC_SOURCE if roofline["traffic"] else "not measured"
 
     if args.trailing:
         # short k: HBM reported beside the issue roofline (algorithmic bytes 4*(mk + kn + 2mn))
@@ -385,12 +385,47 @@ def ours(args):
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {exc}"}
 
+    # bit-exact check of the benched kernel on its own problem: one more step on a copy of
+    # the current C, sampled columns against the reference's own CPU Rgemm (rank 0)
+    if rank == 0 and not args.no_check:
+        line["bit_exact_sample"] = bit_exact_sample(pg, A, lda, B, ldb, C, m, n, k, ta, tb, alpha, beta, ws,
+                                                    stream)
+
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def bit_exact_sample(pg, A, lda, B, ldb, C, m, n, k, ta, tb, alpha, beta, ws, stream, width=8):
+    """One step of the benched GEMM on a copy of C, compared on sampled columns (all
+    rows of the first, middle and last `width` columns) with the reference's own CPU Rgemm
+    (oracle/_ref; the restatement where that was not built)."""
+    import numpy as np
+    import torch
+    try:
+        import oracle  # checker only
+        Cout = C.clone()
+        pg.Rgemm_dev(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cout, m, workspace=ws, stream=stream)
+        torch.cuda.synchronize()
+        hA = A.cpu().numpy().view(np.uint32)
+        hB = B.cpu().numpy().view(np.uint32)
+        hC = C.cpu().numpy().view(np.uint32)
+        got = Cout.cpu().numpy().view(np.uint32)
+        mid = (n // 2) // width * width
+        spans = sorted({(0, min(width, n)), (mid, min(mid + width, n)), (max(0, n - width), n)})
+        t0 = time.perf_counter()
+        bad, kind = 0, None
+        for j0, j1 in spans:
+            want, kind = oracle.rgemm_cols_checked(ta, tb, m, n, k, alpha, hA, lda, hB, ldb, beta, hC, m, j0, j1)
+            bad += int(np.count_nonzero(got[j0 * m:j1 * m] != want))
+        return {"ok": bad == 0, "mismatches": bad, "entries": sum(j1 - j0 for j0, j1 in spans) * m,
+                "columns": [[j0, j1 - 1] for j0, j1 in spans], "checker": kind,
+                "check_s": round(time.perf_counter() - t0, 1)}
+    except Exception as exc:  # reported; a failed check is never hidden
+        return {"ok": False, "error": str(exc)}
 
 
 # ---------------------------------------------------------------------------
@@ -436,7 +471,10 @@ def factor_arm(args):
             pg.Rpotrf_dev("L", n, A, n, info, nb=nb)
 
     times = []
+    sampler = ClockSampler(torch.cuda.current_device())
     for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            sampler.start()
         A.copy_(A0)
         e0, e1 = _events()
         e0.record()
@@ -445,6 +483,7 @@ def factor_arm(args):
         torch.cuda.synchronize()
         if i >= args.warmup:
             times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
     ms = sum(times) / len(times)
     rhs = b.clone()
     e0, e1 = _events()
@@ -490,7 +529,7 @@ def factor_arm(args):
             "data": "synthetic", "config": {"workload": f"{args.workload} n={n} nb={nb}, "
                                                         f"{'U[-1,1]' if lu else 'M*M^T/n + I, M ~ U[-1,1]'}, "
                                                         "one right-hand side b = A*x_true"},
-            "info": int(info.item()), "solve_ms": round(solve_ms, 3), "fp64_report": rep}
+            "info": int(info.item()), "solve_ms": round(solve_ms, 3), "fp64_report": rep, "clocks": clocks}
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -540,7 +579,10 @@ def batch_arm(args):
     plan = pg.BatchPlan([(int(kinds[i]), view(A, offA, i), view(B, offB, i), view(ipiv, offB, i), info[i:i + 1])
                          for i in range(P)])
     times = []
+    sampler = ClockSampler(torch.cuda.current_device())
     for r in range(args.warmup + args.steps):
+        if r == args.warmup:
+            sampler.start()
         A.copy_(A0)
         B.copy_(B0)
         e0, e1 = _events()
@@ -550,6 +592,7 @@ def batch_arm(args):
         torch.cuda.synchronize()
         if r >= args.warmup:
             times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
     batch_ms = sum(times) / len(times)
     # per-call path on a sample (same problems, same order)
     S_ = min(P, 400)
@@ -594,7 +637,10 @@ def batch_arm(args):
 
     gplan = pg.BatchGemmPlan([gprob(i, GC) for i in range(G)], tile_table=autotune.gemm_tile_table())
     gt = []
+    gsampler = ClockSampler(torch.cuda.current_device())
     for r in range(args.warmup + args.steps):
+        if r == args.warmup:
+            gsampler.start()
         GC.copy_(GC0)
         e0, e1 = _events()
         e0.record()
@@ -603,6 +649,7 @@ def batch_arm(args):
         torch.cuda.synchronize()
         if r >= args.warmup:
             gt.append(e0.elapsed_time(e1))
+    gclocks = gsampler.stop()
     gbatch_ms = sum(gt) / len(gt)
     ops = float(np.sum(2.0 * gm * gn * gk))
     GS = min(G, 2000)
@@ -632,8 +679,8 @@ def batch_arm(args):
                            "per_call_gop_s": round(ops_s / (gpercall_ms / 1e3) / 1e9, 2),
                            "per_call_gemms_per_s": round(GS / (gpercall_ms / 1e3), 1), "per_call_sample": GS,
                            "bit_identical_to_per_call_on_sample": bool(gsame),
-                           "tile_table": autotune.gemm_tile_table()},
-            "max_info": int(info.max().item())}
+                           "tile_table": autotune.gemm_tile_table(), "clocks": gclocks},
+            "max_info": int(info.max().item()), "clocks": clocks}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -152,3 +152,27 @@ def rgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, cols=None):
     if cols is None:
         return orc.orc_rgemm(*args)
     return orc.orc_rgemm_cols(*args, cols[0], cols[1])
+
+
+def rgemm_cols_checked(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, j0, j1):
+    """Columns j0..j1-1 of the Rgemm result, computed by the reference's own compiled
+    Rgemm (``ref``) where it was built, else by the restatement: returns a copy of those
+    columns of C (ldc x (j1 - j0), flat) after the update, and which checker ran.
+
+    Columns of C are independent in every order of Rgemm.cpp:163-247, so the reference
+    routine runs on the slice: op(B)'s columns j0..j1-1 start at B[j0*ldb] ('N') or at
+    B[j0] ('T'/'C', B is n x k), and C's at C[j0*ldc]."""
+    A = np.ascontiguousarray(A, dtype=np.uint32)
+    B = np.ascontiguousarray(B, dtype=np.uint32)
+    Cs = np.array(C[j0 * ldc:j1 * ldc], dtype=np.uint32, copy=True)
+    w = j1 - j0
+    if ref is not None:
+        Bs = B[j0 * ldb:] if tb in "nN" else B[j0:]
+        ref.ref_rgemm(ta.encode(), tb.encode(), m, w, k, alpha, A, lda, np.ascontiguousarray(Bs), ldb,
+                      beta, Cs, ldc)
+        return Cs, "reference"
+    Cf = np.array(C, dtype=np.uint32, copy=True)
+    rc = orc.orc_rgemm_cols(ta.encode(), tb.encode(), m, n, k, alpha, A, lda, B, ldb, beta, Cf, ldc, j0, j1)
+    if rc != 0:
+        raise ValueError(f"oracle Rgemm info {rc}")
+    return Cf[j0 * ldc:j1 * ldc].copy(), "port"

@@ -15,7 +15,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DEFAULT = "/root/reference"
+# The reference tree: $POSIT_REFERENCE_DIR, else a directory named "reference" beside this
+# repository's root.
+REF_DEFAULT = os.environ.get("POSIT_REFERENCE_DIR") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 # The reference CPU routines on the GEMM / LU / Cholesky path (libRpack/Makefile:15-21
 # minus the OpenCL glue, iMlaenv (replaced) and util.cpp (LAPACK generators)).
 REF_SOURCES = [

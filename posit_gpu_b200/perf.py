@@ -10,6 +10,9 @@ multiply-add is a property of the compiled kernel (its fast path is branch-free)
 measured with ncu on the same kernel and recorded here.
 """
 
+import hashlib
+import os
+
 SM_COUNT = 148
 SMSP_PER_SM = 4
 SM_MAX_MHZ = 1965.0
@@ -35,3 +38,37 @@ def issue_peak_warp_inst_per_s(sm_mhz):
 def fp64_pipe_peak_warp_inst_per_s(sm_mhz):
     """FP64 pipe: 16 lanes per SM sub-partition per cycle, i.e. half a warp instruction."""
     return SM_COUNT * SMSP_PER_SM * 0.5 * float(sm_mhz) * 1e6
+
+
+# The instruction count above belongs to one build of the main kernel.  It is tied to
+# that build by a SHA-256 over the sources that define the kernel's instruction stream and
+# the script that compiles them (flags included); the benchmark recomputes the digest and,
+# when it differs, marks the count stale and reports no roofline fraction from it.
+KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh", "build.py"]
+INST_SOURCE_DIGEST = None
+
+
+def kernel_source_digest():
+    here = os.path.dirname(os.path.abspath(__file__))
+    h = hashlib.sha256()
+    for rel in KERNEL_SOURCES:
+        with open(os.path.join(here, rel), "rb") as fh:
+            h.update(rel.encode() + b"\0" + fh.read() + b"\0")
+    return h.hexdigest()
+
+
+def inst_count_current():
+    """True when WARP_INST_PER_MAD was measured on the kernel sources present now."""
+    return INST_SOURCE_DIGEST is not None and kernel_source_digest() == INST_SOURCE_DIGEST
+
+
+# DRAM bytes (read + write) of one main-kernel launch at the LU trailing-update shapes
+# m = n = 8192 - b, k = b (key b), from ncu dram__bytes_read.sum + dram__bytes_write.sum
+# of that launch.  Empty until measured; the benchmark then reports no traffic figure for
+# the shape rather than one scaled from another shape.
+TRAILING_TRAFFIC_BYTES = {}
+TRAILING_TRAFFIC_SOURCE = None
+
+
+def trailing_traffic(k):
+    return TRAILING_TRAFFIC_BYTES.get(int(k))

@@ -155,3 +155,22 @@ def test_div_sqrt_correctly_rounded():
     assert o.orc_p32_div(0x40000000, 0) == 0x80000000
     assert o.orc_p32_sqrt(0xC0000000) == 0x80000000
     assert o.orc_p32_sqrt(0x40000000) == 0x40000000
+
+
+def test_column_slice_checker_matches_whole_rgemm():
+    """oracle.rgemm_cols_checked (the reference's Rgemm on a slice of C's columns) equals
+    the same columns of the whole restated Rgemm, for every transpose case."""
+    rng = np.random.default_rng(1)
+    for ta, tb in (("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")):
+        m, n, k = 37, 29, 23
+        ar = m if ta == "N" else k
+        br = k if tb == "N" else n
+        A = oracle.from_double(rng.uniform(-1, 1, m * k))
+        B = oracle.from_double(rng.uniform(-1, 1, k * n))
+        C = oracle.from_double(rng.uniform(-1, 1, m * n))
+        full = C.copy()
+        oracle.rgemm(ta, tb, m, n, k, oracle.P32_MINUS_ONE, A, ar, B, br, oracle.p32(0.5), full, m)
+        for j0, j1 in ((0, 5), (10, 29), (28, 29)):
+            got, _ = oracle.rgemm_cols_checked(ta, tb, m, n, k, oracle.P32_MINUS_ONE, A, ar, B, br,
+                                               oracle.p32(0.5), C, m, j0, j1)
+            assert np.array_equal(got, full[j0 * m:j1 * m]), (ta, tb, j0)
