@@ -26,7 +26,7 @@ extern "C" {
 #define POSIT_E_DEVICE_FAULT (-4) /* a kernel raised its error flag (bounded wait expired) */
 #define POSIT_E_WORKSPACE (-5)    /* caller-provided workspace too small */
 #define POSIT_E_NOALLOC_LIMIT (-6) /* shape needs more scratch than posit_rgemm_dev_noalloc has */
-#define POSIT_E_UNSUPPORTED (-7)   /* a variant this library does not implement on the device */
+#define POSIT_E_UNSUPPORTED (-7)   /* reserved: a variant this library does not implement on the device */
 
 /* Replaces initOpenCL (libRpack/def.h:63, libRpack/Rgemm_opencl.cpp:59-70): selects
  * the current CUDA device, creates its context and warms the kernels.  Optional: every
@@ -87,12 +87,17 @@ size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
  * the reference does, and its factors stay bit-identical; a Cholesky factorization that
  * stops (info > 0) leaves the not-yet-factored part of A in an unspecified state (the
  * reference's left-looking blocking and this right-looking one differ there).
- * nb <= 0 selects 256.
+ * nb <= 0 selects 256.  Upper Cholesky is the exception: in the reference's order
+ * (left-looking, each entry's update a dot product over the rows above it, Rpotrf.cpp:96-118)
+ * its bits depend on nb, which is therefore the caller's -- the reference CPU routine's
+ * own block size comes from iMlaenv, 64 (iMlaenv.cpp:223-228), and nb <= 0 selects that.
  *
  * _dev forms: device pointers (ipiv and info included: *info is written on the device,
  * asynchronously on `stream`); workspace is stream-ordered.  Host forms: host pointers,
- * synchronous.  Only trans = 'N' (Rgetrs) and uplo = 'L' (Rpotrf/Rpotrs) run on the
- * device; the others return POSIT_E_UNSUPPORTED. */
+ * synchronous.  Every variant runs on the device: Rgetrs with trans 'N', 'T' or 'C'
+ * (Rgetrs.cpp:84-113), Rpotrf and Rpotrs with uplo 'L' or 'U' (Rpotrf.cpp:96-143,
+ * Rpotrs.cpp:84-106). */
+#define POSIT_RPOTRF_UPPER_DEFAULT_NB 64
 
 /* Rgetrf (libRpack/Rgetrf.cpp:32-137; mplapack_posit.h:48), Rgetrf_opencl (mplapack_posit.h:49) */
 int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream);

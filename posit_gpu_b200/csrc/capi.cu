@@ -248,14 +248,15 @@ int posit_rgetrs_dev(char trans, int n, int nrhs, const uint32_t *A, int lda, co
         return 5;
     if (ldb < imax(1, n))
         return 8;
-    if (!notr)
-        return POSIT_E_UNSUPPORTED;
     int r = ensure_init();
     if (r)
         return r;
     if (n == 0 || nrhs == 0)
         return 0;
-    PG_TRY(pg::rgetrs_launch(n, nrhs, A, lda, ipiv, B, ldb, as_stream(stream)));
+    if (notr)
+        PG_TRY(pg::rgetrs_launch(n, nrhs, A, lda, ipiv, B, ldb, as_stream(stream)));
+    else
+        PG_TRY(pg::rgetrs_trans_launch(n, nrhs, A, lda, ipiv, B, ldb, as_stream(stream)));
     return 0;
 }
 
@@ -268,8 +269,6 @@ int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, 
         return 2;
     if (lda < imax(1, n))
         return 4;
-    if (upper)
-        return POSIT_E_UNSUPPORTED;
     int r = ensure_init();
     if (r)
         return r;
@@ -277,11 +276,16 @@ int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, 
     PG_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
     if (n == 0)
         return 0;
-    nb = pick_nb(nb);
+    // the upper factor depends on nb: the default is the reference's own block size
+    nb = upper ? (nb > 0 ? nb : POSIT_RPOTRF_UPPER_DEFAULT_NB) : pick_nb(nb);
+    const size_t wsb = upper ? pg::rpotrf_upper_workspace_bytes(n, nb) : pg::rpotrf_workspace_bytes(n, nb);
     void *ws = nullptr;
-    PG_TRY(cudaMallocAsync(&ws, pg::rpotrf_workspace_bytes(n, nb), st));
-    cudaError_t e = pg::rpotrf_lower_launch(n, A, lda, nb, info, ws, st);
-    cudaFreeAsync(ws, st);
+    if (wsb)
+        PG_TRY(cudaMallocAsync(&ws, wsb, st));
+    cudaError_t e = upper ? pg::rpotrf_upper_launch(n, A, lda, nb, info, ws, st)
+                          : pg::rpotrf_lower_launch(n, A, lda, nb, info, ws, st);
+    if (ws)
+        cudaFreeAsync(ws, st);
     return e == cudaSuccess ? 0 : cuda_fail(e);
 }
 
@@ -298,14 +302,15 @@ int posit_rpotrs_dev(char uplo, int n, int nrhs, const uint32_t *A, int lda, uin
         return 5;
     if (ldb < imax(1, n))
         return 7;
-    if (upper)
-        return POSIT_E_UNSUPPORTED;
     int r = ensure_init();
     if (r)
         return r;
     if (n == 0 || nrhs == 0)
         return 0;
-    PG_TRY(pg::rpotrs_lower_launch(n, nrhs, A, lda, B, ldb, as_stream(stream)));
+    if (upper)
+        PG_TRY(pg::rpotrs_upper_launch(n, nrhs, A, lda, B, ldb, as_stream(stream)));
+    else
+        PG_TRY(pg::rpotrs_lower_launch(n, nrhs, A, lda, B, ldb, as_stream(stream)));
     return 0;
 }
 
@@ -370,8 +375,6 @@ int posit_rgetrs(char trans, int n, int nrhs, const uint32_t *A, int lda, const 
         return 5;
     if (ldb < imax(1, n))
         return 8;
-    if (!notr)
-        return POSIT_E_UNSUPPORTED;
     if (n == 0 || nrhs == 0)
         return 0;
     int r = ensure_init();
@@ -408,8 +411,6 @@ int posit_rpotrf(char uplo, int n, uint32_t *A, int lda, int nb, int *info)
         return 2;
     if (lda < imax(1, n))
         return 4;
-    if (upper)
-        return POSIT_E_UNSUPPORTED;
     *info = 0;
     if (n == 0)
         return 0;
@@ -449,8 +450,6 @@ int posit_rpotrs(char uplo, int n, int nrhs, const uint32_t *A, int lda, uint32_
         return 5;
     if (ldb < imax(1, n))
         return 7;
-    if (upper)
-        return POSIT_E_UNSUPPORTED;
     if (n == 0 || nrhs == 0)
         return 0;
     int r = ensure_init();

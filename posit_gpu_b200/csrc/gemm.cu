@@ -171,11 +171,12 @@ __global__ void decode_b_kernel(bool notb, int k, int n, const uint32_t *__restr
 // ---------------------------------------------------------------------------
 // Main kernel
 // ---------------------------------------------------------------------------
-// LOWER: only entries with row >= column are written (tiles wholly above the diagonal
-// exit at once) -- the symmetric trailing update of a lower Cholesky factorization.
+// TRI selects the entries written: TRI_FULL all of C; TRI_LOWER only row >= column (the
+// symmetric trailing update of a lower Cholesky factorization); TRI_UPPER only row <=
+// column (Rsyrk('U', 'T') of an upper one).  Tiles wholly outside the triangle exit at once.
 // `stop`, if given, is a device flag (a factorization's info) that turns the call into a
 // no-op when it is nonzero.
-template <bool DOT, bool LOWER>
+template <bool DOT, int TRI>
 __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     gemm_main_kernel(int m, int n, int k, int KT, uint32_t alpha, uint32_t beta,
                      const double *__restrict__ Ad, const double *__restrict__ Td, uint32_t *__restrict__ C,
@@ -184,8 +185,10 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
 {
     if (stop && *stop != 0)
         return;
-    if (LOWER && (int)(blockIdx.x * BM + BM - 1) < (int)(blockIdx.y * BN))
+    if (TRI == TRI_LOWER && (int)(blockIdx.x * BM + BM - 1) < (int)(blockIdx.y * BN))
         return; // every row of the tile is above its first column
+    if (TRI == TRI_UPPER && (int)(blockIdx.x * BM) > (int)(blockIdx.y * BN + BN - 1))
+        return; // every row of the tile is below its last column
     extern __shared__ __align__(128) unsigned char smem_raw[];
     double *As = reinterpret_cast<double *>(smem_raw);
     double *Ts = As + STAGES * BK * BM;
@@ -282,7 +285,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int row = mt * BM + own_off(tx, i), col = nt * BN + own_off(ty, j);
-            if (row < m && col < n && (!LOWER || row >= col)) {
+            if (row < m && col < n && (TRI != TRI_LOWER || row >= col) && (TRI != TRI_UPPER || row <= col)) {
                 uint32_t *cp = C + (size_t)row + (size_t)col * ldc;
                 const bool nar = ((nar_bits >> (i * TN + j)) & 1u) || row_nar[row] || col_nar[col];
                 uint32_t v = nar ? P32_NAR : p32_from_double(acc[i][j]);
@@ -398,7 +401,7 @@ static int grid_for(size_t total, int threads)
     return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
-template <bool LOWER>
+template <int TRI>
 static cudaError_t gemm_launch_impl(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
                                     int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
                                     void *workspace, cudaStream_t stream, const int *stop)
@@ -418,19 +421,19 @@ static cudaError_t gemm_launch_impl(bool nota, bool notb, int m, int n, int k, u
                                                            Td, col_nar);
     const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(double) + (size_t)F64_CONST_ENTRIES * sizeof(uint32_t);
     dim3 grid(p.mt, p.nt);
-    e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem)
-            : cudaFuncSetAttribute(gemm_main_kernel<false, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            : cudaFuncSetAttribute(gemm_main_kernel<false, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem);
     if (e != cudaSuccess)
         return e;
     const bool prof = g_prof_on;
     cudaEvent_t e0 = prof ? prof_mark(stream) : nullptr;
     if (dot)
-        gemm_main_kernel<true, LOWER><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
+        gemm_main_kernel<true, TRI><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
                                                                         (size_t)ldc, row_nar, col_nar, stop);
     else
-        gemm_main_kernel<false, LOWER><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
+        gemm_main_kernel<false, TRI><<<grid, NTHREADS, smem, stream>>>(m, n, k, p.kt, alpha, beta, Ad, Td, C,
                                                                          (size_t)ldc, row_nar, col_nar, stop);
     if (prof) {
         cudaEvent_t e1 = prof_mark(stream);
@@ -445,16 +448,30 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
                         const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *workspace,
                         cudaStream_t stream)
 {
-    return gemm_launch_impl<false>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
-                                   nullptr);
+    return gemm_launch_impl<TRI_FULL>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
+                                      nullptr);
+}
+
+cudaError_t gemm_launch_tri(int tri, bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A,
+                            int lda, const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc,
+                            void *workspace, cudaStream_t stream, const int *stop)
+{
+    if (tri == TRI_LOWER)
+        return gemm_launch_impl<TRI_LOWER>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace,
+                                           stream, stop);
+    if (tri == TRI_UPPER)
+        return gemm_launch_impl<TRI_UPPER>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace,
+                                           stream, stop);
+    return gemm_launch_impl<TRI_FULL>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
+                                      stop);
 }
 
 cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_t alpha, const uint32_t *A, int lda,
                               const uint32_t *B, int ldb, uint32_t beta, uint32_t *C, int ldc, void *workspace,
                               cudaStream_t stream, const int *stop)
 {
-    return gemm_launch_impl<true>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace, stream,
-                                  stop);
+    return gemm_launch_impl<TRI_LOWER>(nota, notb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, workspace,
+                                       stream, stop);
 }
 
 cudaError_t scale_launch(int m, int n, bool dot, uint32_t alpha, uint32_t beta, uint32_t *C, int ldc,

@@ -18,6 +18,11 @@ constexpr int STAGES = 3;
 constexpr int MIN_CTAS_PER_SM = 4;
 static_assert(TM % 2 == 0 && TN % 2 == 0, "operands are loaded in pairs");
 
+// Which entries of C a launch writes (gemm_launch_tri).
+constexpr int TRI_FULL = 0;
+constexpr int TRI_LOWER = 1; // row >= column
+constexpr int TRI_UPPER = 2; // row <= column
+
 // Error flags a kernel can raise (read back with posit_get_device_error).
 constexpr int DEV_ERR_WAIT_TIMEOUT = 1;
 
@@ -45,6 +50,12 @@ cudaError_t gemm_launch(bool nota, bool notb, int m, int n, int k, uint32_t alph
 cudaError_t gemm_launch_lower(bool nota, bool notb, int m, int n, int k, uint32_t alpha,
                               const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
                               uint32_t *C, int ldc, void *workspace, cudaStream_t stream, const int *stop);
+
+// Any of the three: all of C, its lower or its upper triangle (TRI_*), doing nothing when
+// *stop != 0 (stop may be null).
+cudaError_t gemm_launch_tri(int tri, bool nota, bool notb, int m, int n, int k, uint32_t alpha,
+                            const uint32_t *A, int lda, const uint32_t *B, int ldb, uint32_t beta,
+                            uint32_t *C, int ldc, void *workspace, cudaStream_t stream, const int *stop);
 
 // The calls that form no product (alpha == 0, or k == 0), on the m x n submatrix:
 // C <- 0 or beta*C; with `dot` (TN/TT and k == 0, alpha != 0) C <- alpha*0 or

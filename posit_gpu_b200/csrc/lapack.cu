@@ -24,6 +24,8 @@
 // dependent) is not implemented on the device.
 #include "gemm.cuh"
 #include "lapack.cuh"
+
+#include <algorithm>
 #include "posit32.cuh"
 #include "trsm_chain.cuh"
 
@@ -180,6 +182,112 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
     for (int j = 0; j < cn; ++j) { // a_ic + (-u_kc)*l_i in the FP64 step (posit32.cuh)
         uint32_t *pc = P + i + (size_t)(c0 + j) * lda;
         *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_u[j], dl));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LU panel in one CTA (panels of at most PANEL1_MAX_M rows): the same per-column steps as
+// lu_pivot_kernel + lu_update_kernel -- iRamax with first-max tie-break, the interchange
+// across the panel, the scaling decision, the scaled column, the rank-1 update in the FP64
+// step -- in the same per-element order, with a barrier between steps instead of a kernel
+// boundary, so a whole panel is one launch.  For short panels the two launches per column
+// (a few microseconds each) cost more than the arithmetic; for tall ones the
+// many-block update wins, so the host picks by the panel height.
+// ---------------------------------------------------------------------------
+constexpr int PANEL1_THREADS = 1024;
+constexpr int PANEL1_MAX_JB = 512;
+constexpr int PANEL1_MAX_M = 4096;
+
+__global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cta_kernel(uint32_t *__restrict__ P, size_t lda, int M,
+                                                                      int jb, int row0, int *__restrict__ ipiv,
+                                                                      int *__restrict__ info)
+{
+    __shared__ int32_t s_key[32];
+    __shared__ int s_idx[32];
+    __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row, FP64
+    __shared__ PivotInfo s_pi;
+    if (*info < 0)
+        return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = 0; k < jb; ++k) {
+        const uint32_t *col = P + (size_t)k * lda;
+        // iRamax over rows [k, M) (iRamax.cpp:65-71), as in lu_pivot_kernel
+        int32_t best = INT32_MIN;
+        int bidx = -1;
+        for (int i = k + tid; i < M; i += PANEL1_THREADS) {
+            const int32_t key = (int32_t)pabs(col[i]);
+            if (bidx < 0 || key > best) {
+                best = key;
+                bidx = i;
+            }
+        }
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const int32_t k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
+                const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
+                if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
+                    best = k2;
+                    bidx = i2;
+                }
+            }
+            if (round == 0) {
+                if (lane == 0) {
+                    s_key[warp] = best;
+                    s_idx[warp] = bidx;
+                }
+                __syncthreads();
+                best = s_key[lane];
+                bidx = s_idx[lane];
+            }
+        }
+        if (tid == 0) {
+            const int p = bidx;
+            const uint32_t piv = col[p];
+            ipiv[row0 + k] = row0 + p + 1; // 1-based, global
+            PivotInfo pi;
+            pi.row = p;
+            pi.piv = piv;
+            if (piv == 0) {
+                pi.mode = 0;
+                pi.recip = 0;
+                if (*info == 0)
+                    *info = row0 + k + 1;
+            } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
+                pi.mode = 1;
+                pi.recip = pdiv(P32_ONE, piv);
+            } else {
+                pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
+                pi.recip = 0;
+            }
+            s_pi = pi;
+        }
+        __syncthreads();
+        const PivotInfo pi = s_pi;
+        if (pi.piv != 0 && pi.row != k) { // interchange rows k and p across the panel (Rgetrf2.cpp:107-117)
+            for (int c = tid; c < jb; c += PANEL1_THREADS) {
+                uint32_t *pc = P + (size_t)c * lda;
+                const uint32_t t = pc[k];
+                pc[k] = pc[pi.row];
+                pc[pi.row] = t;
+            }
+        }
+        __syncthreads();
+        for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
+            s_u[c] = -p32_to_double(P[k + (size_t)c * lda]);
+        __syncthreads();
+        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS) {
+            uint32_t *pik = P + i + (size_t)k * lda;
+            const uint32_t l = lu_scaled(*pik, pi);
+            *pik = l;
+            const double dl = p32_to_double(l);
+            for (int c = k + 1; c < jb; ++c) { // a_ic + (-u_kc)*l_i in the FP64 step
+                uint32_t *pc = P + i + (size_t)c * lda;
+                *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_u[c], dl));
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -358,22 +466,22 @@ constexpr int LLT_SMEM_MAX = 227 * 1024;
 
 __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict__ L, size_t ldl,
                                                       uint32_t *__restrict__ B, size_t ldb, int m, bool staged,
-                                                      bool unit, const int *__restrict__ info)
+                                                      bool unit, bool upper, const int *__restrict__ info)
 {
     extern __shared__ uint32_t s_col[];
-    if (info && *info < 0)
+    if (info && *info != 0) // a factorization stopped before this solve
         return;
     uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
     if (!staged) {
         if (threadIdx.x == 0)
-            llt_chain(L, ldl, bcol, m, unit);
+            llt_chain(L, ldl, bcol, m, unit, upper);
         return;
     }
     for (int i = threadIdx.x; i < m; i += 32)
         s_col[i] = bcol[i];
     __syncwarp();
     if (threadIdx.x == 0)
-        llt_chain(L, ldl, s_col, m, unit);
+        llt_chain(L, ldl, s_col, m, unit, upper);
     __syncwarp();
     for (int i = threadIdx.x; i < m; i += 32)
         bcol[i] = s_col[i];
@@ -487,7 +595,11 @@ struct LltTerms<uint32_t> {
     __device__ static uint32_t store(uint32_t p) { return p; }
 };
 
-template <class T>
+// UPPER: the same solve for an upper triangle, U^-T b (Rtrsm('L', 'U', 'T'),
+// Rtrsm.cpp:160-173), rows in increasing order: row i sums its terms k = 0 .. i-1 in
+// ascending order, so the warp scans the terms k <= i-2 (computed while row i-1 ran) and
+// then adds the last one, -u_{i-1,i} * b_{i-1}, from the value just finished.
+template <class T, bool UPPER = false>
 __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint32_t *__restrict__ L, size_t ldl,
                                                                      uint32_t *__restrict__ B, size_t ldb, int m,
                                                                      bool unit, const int *__restrict__ info)
@@ -496,7 +608,7 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
     T *s_q = reinterpret_cast<T *>(smem_pc); // [2][m]: terms
     uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
     __shared__ uint32_t s_nar[2];
-    if (info && *info < 0)
+    if (info && *info != 0) // a factorization stopped before this solve
         return;
     uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
     const int tid = threadIdx.x;
@@ -505,17 +617,23 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
     if (tid < 2)
         s_nar[tid] = 0;
     __syncthreads();
-    uint32_t xprev = 0; // b_{i+1}, final (warp 0)
-    for (int i = m - 1; i >= 0; --i) {
-        const int cur = i & 1;
+    uint32_t xprev = 0; // the row finished last, b_{i+1} (lower) or b_{i-1} (upper) (warp 0)
+    for (int step = 0; step < m; ++step) {
+        const int i = UPPER ? step : m - 1 - step;
+        const int cur = step & 1;
         if (tid < 32) {
             const uint32_t *li = L + (size_t)i * ldl;
             const uint32_t bi = s_b[i];
             uint32_t nar = (bi == P32_NAR) | s_nar[cur];
             double c = p32_to_double(bi == P32_NAR ? 0u : bi);
-            if (i + 1 < m) {
+            const typename LltTerms<T>::View q{s_q + (size_t)cur * m};
+            if (!UPPER && i + 1 < m) {
                 c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
-                c = warp_chain_scan<LLT_SCAN_E>(c, typename LltTerms<T>::View{s_q + (size_t)cur * m}, i + 2, m);
+                c = warp_chain_scan<LLT_SCAN_E>(c, q, i + 2, m);
+            }
+            if (UPPER && i >= 1) {
+                c = warp_chain_scan<LLT_SCAN_E>(c, q, 0, i - 1);
+                c = chain_add_one(c, llt_term(li[i - 1], xprev, &nar));
             }
             uint32_t t = nar ? P32_NAR : p32_from_double(c);
             if (!unit)
@@ -526,12 +644,15 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
                 s_b[i] = t;
                 s_nar[cur] = 0;
             }
-        } else if (i >= 1) {
-            // terms k = i+1 .. m-1 of row i-1 (their b_k are final)
-            const uint32_t *lp = L + (size_t)(i - 1) * ldl;
+        } else if (step + 1 < m) {
+            // the terms of the next row whose b_k are final: k = i+1 .. m-1 of row i-1
+            // (lower), k = 0 .. i-1 of row i+1 (upper)
+            const int nxt = UPPER ? i + 1 : i - 1;
+            const int kbeg = UPPER ? 0 : i + 1, kend = UPPER ? i : m;
+            const uint32_t *lp = L + (size_t)nxt * ldl;
             T *qn = s_q + (size_t)(cur ^ 1) * m;
             uint32_t nar = 0;
-            for (int k = i + 1 + (tid - 32); k < m; k += LLT_PC_THREADS - 32) {
+            for (int k = kbeg + (tid - 32); k < kend; k += LLT_PC_THREADS - 32) {
                 const uint32_t p = pmul(0u - s_b[k], lp[k]); // (-b)*a == -(a*b) bit for bit
                 nar |= p == P32_NAR;
                 qn[k] = LltTerms<T>::store(p == P32_NAR ? 0u : p);
@@ -628,6 +749,163 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
     }
 }
 
+// Lower Cholesky panel in one CTA, the counterpart of chol_diag_kernel +
+// chol_update_kernel: per column the square root and reciprocal of the diagonal
+// (Rpotrf2.cpp:90-97), the column below it times the reciprocal (Rtrsm.cpp:265-268), the
+// rank-1 update of the lower part of the rest of the panel, with barriers in between.
+__global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cta_kernel(uint32_t *__restrict__ P, size_t lda,
+                                                                        int M, int jb, int row0,
+                                                                        int *__restrict__ info)
+{
+    __shared__ double s_l[PANEL1_MAX_JB]; // -l_ck of the current column, FP64
+    __shared__ uint32_t s_recip;
+    __shared__ int s_stop;
+    if (*info != 0)
+        return;
+    const int tid = threadIdx.x;
+    for (int k = 0; k < jb; ++k) {
+        uint32_t *pk = P + (size_t)k * lda;
+        if (tid == 0) {
+            const uint32_t akk = pk[k];
+            s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
+            if (s_stop) {
+                *info = row0 + k + 1;
+            } else {
+                const uint32_t lkk = psqrt(akk);
+                s_recip = pdiv(P32_ONE, lkk);
+                pk[k] = lkk;
+            }
+        }
+        __syncthreads();
+        if (s_stop)
+            return;
+        const uint32_t recip = s_recip;
+        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS)
+            pk[i] = pmul(recip, pk[i]);
+        __syncthreads();
+        for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
+            s_l[c] = -p32_to_double(pk[c]);
+        __syncthreads();
+        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS) {
+            const double dl = p32_to_double(pk[i]);
+            const int cend = min(jb - 1, i);
+            for (int c = k + 1; c <= cend; ++c) { // a_ic + (-l_ck)*l_i in the FP64 step
+                uint32_t *pc = P + i + (size_t)c * lda;
+                *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_l[c], dl));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Upper Cholesky diagonal block: Rpotrf2('U') (Rpotrf2.cpp:86-131) in one CTA
+// ---------------------------------------------------------------------------
+// The recursion exactly as the reference runs it, since the upper factor's bits depend on
+// how the work is grouped: a 1x1 block takes the square root (a <= 0, NaR included, stops
+// with info); a larger one splits n1 = n/2, n2 = n - n1, factors A11, solves
+// A12 <- U11^-T A12 (Rtrsm('L', 'U', 'T', 'N'), Rtrsm.cpp:160-173: per column, for each
+// row i, t = b_i, t = t - u_ki*b_k over k < i in order, b_i = t / u_ii), updates
+// A22 <- -(A12^T A12) + A22 on and above the diagonal (Rsyrk('U', 'T'), Rsyrk.cpp:182-195:
+// each entry's dot product summed from zero in order, then alpha*t + beta*c) and factors
+// A22.  The recursion runs on an explicit stack in shared memory; the solves are one
+// thread per column, the update one thread per entry, with barriers in between.
+constexpr int POTRF2_CTA_THREADS = 256;
+constexpr int POTRF2_CTA_MAX = 128; // larger blocks recurse on the host with many-block kernels
+
+__global__ void __launch_bounds__(POTRF2_CTA_THREADS) potrf2_upper_cta_kernel(uint32_t *__restrict__ A, size_t lda,
+                                                                              int n, int row0, int *__restrict__ info)
+{
+    constexpr int DEPTH = 16;
+    __shared__ int s_off[DEPTH], s_n[DEPTH], s_stage[DEPTH];
+    __shared__ int s_sp, s_stop;
+    if (*info != 0)
+        return;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_sp = 1;
+        s_off[0] = 0;
+        s_n[0] = n;
+        s_stage[0] = 0;
+        s_stop = 0;
+    }
+    __syncthreads();
+    for (;;) {
+        const int sp = s_sp;
+        if (sp == 0)
+            break;
+        const int off = s_off[sp - 1], nn = s_n[sp - 1], stage = s_stage[sp - 1];
+        __syncthreads(); // the frame is read before thread 0 changes the stack
+        if (nn == 1) {
+            if (tid == 0) {
+                uint32_t *d = A + off + (size_t)off * lda;
+                const uint32_t a = *d;
+                if ((int32_t)a <= 0) { // Rpotrf2.cpp:90-93 (NaR is below zero in posit order)
+                    *info = row0 + off + 1;
+                    s_stop = 1;
+                } else {
+                    *d = psqrt(a);
+                }
+                s_sp = sp - 1;
+            }
+        } else {
+            const int n1 = nn / 2, n2 = nn - n1;
+            uint32_t *a11 = A + off + (size_t)off * lda;
+            uint32_t *a12 = A + off + (size_t)(off + n1) * lda;
+            uint32_t *a22 = A + (off + n1) + (size_t)(off + n1) * lda;
+            if (stage == 0) {
+                if (tid == 0) {
+                    s_stage[sp - 1] = 1;
+                    s_off[sp] = off;
+                    s_n[sp] = n1;
+                    s_stage[sp] = 0;
+                    s_sp = sp + 1;
+                }
+            } else if (stage == 1) {
+                for (int j = tid; j < n2; j += POTRF2_CTA_THREADS) { // A12 <- U11^-T A12
+                    uint32_t *b = a12 + (size_t)j * lda;
+                    for (int i = 0; i < n1; ++i) {
+                        const uint32_t *ui = a11 + (size_t)i * lda;
+                        double t = p32_to_double(b[i]);
+                        for (int k = 0; k < i; ++k)
+                            t = f64_posit_mac_checked(t, -p32_to_double(b[k]), p32_to_double(ui[k]));
+                        b[i] = pdiv(p32_from_double(t), ui[i]);
+                    }
+                }
+                __syncthreads();
+                const int cnt = n2 * (n2 + 1) / 2; // A22 <- -(A12^T A12) + A22, i <= j
+                for (int e = tid; e < cnt; e += POTRF2_CTA_THREADS) {
+                    int j = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f); // e = j(j+1)/2 + i
+                    while (j * (j + 1) / 2 > e)
+                        --j;
+                    while ((j + 1) * (j + 2) / 2 <= e)
+                        ++j;
+                    const int i = e - j * (j + 1) / 2;
+                    const uint32_t *ci = a12 + (size_t)i * lda, *cj = a12 + (size_t)j * lda;
+                    double t = 0.0;
+                    for (int l = 0; l < n1; ++l)
+                        t = f64_posit_mac_checked(t, p32_to_double(ci[l]), p32_to_double(cj[l]));
+                    uint32_t *c = a22 + i + (size_t)j * lda;
+                    *c = padd(pmul(0xC0000000u /* -1 */, p32_from_double(t)), pmul(P32_ONE, *c));
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    s_stage[sp - 1] = 2;
+                    s_off[sp] = off + n1;
+                    s_n[sp] = n2;
+                    s_stage[sp] = 0;
+                    s_sp = sp + 1;
+                }
+            } else if (tid == 0) {
+                s_sp = sp - 1;
+            }
+        }
+        __syncthreads();
+        if (s_stop)
+            return;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host orchestration
 // ---------------------------------------------------------------------------
@@ -667,10 +945,14 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         const int M = m - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j; // indexed by panel-local row
-        lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, 0, j, ipiv, info, pinfo, lc, -1);
-        for (int k = 0; k < jb; ++k) {
-            lu_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, pinfo, lc);
-            lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k + 1, j, ipiv, info, pinfo, lc, k);
+        if (M <= PANEL1_MAX_M && jb <= PANEL1_MAX_JB) {
+            lu_panel_cta_kernel<<<1, PANEL1_THREADS, 0, st>>>(P, L, M, jb, j, ipiv, info);
+        } else {
+            lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, 0, j, ipiv, info, pinfo, lc, -1);
+            for (int k = 0; k < jb; ++k) {
+                lu_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, pinfo, lc);
+                lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k + 1, j, ipiv, info, pinfo, lc, k);
+            }
         }
         if (j > 0)
             laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
@@ -716,10 +998,14 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         const int M = n - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j;
-        chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, 0, j, info, sync, lc, -1);
-        for (int k = 0; k < jb; ++k) {
-            chol_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, sync, lc);
-            chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, k + 1, j, info, sync, lc, k);
+        if (M <= PANEL1_MAX_M && jb <= PANEL1_MAX_JB) {
+            chol_panel_cta_kernel<<<1, PANEL1_THREADS, 0, st>>>(P, L, M, jb, j, info);
+        } else {
+            chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, 0, j, info, sync, lc, -1);
+            for (int k = 0; k < jb; ++k) {
+                chol_update_kernel<<<panel_grid(M, jb, k), PANEL_ROWS, 0, st>>>(P, L, M, jb, k, info, sync, lc);
+                chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, k + 1, j, info, sync, lc, k);
+            }
         }
         if (j + jb < n) {
             const int nr = n - j - jb;
@@ -729,6 +1015,94 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
             if (e != cudaSuccess)
                 return e;
         }
+    }
+    return cudaGetLastError();
+}
+
+// Upper Cholesky (Rpotrf.cpp:96-118): left-looking and blocked by nb in the reference's
+// order, which the upper factor's bits depend on.  For each block column j: the diagonal
+// block's update by the rows above it (Rsyrk('U', 'T'): the TN GEMM on its upper
+// triangle), its factorization (Rpotrf2('U'), recursive), the block row's update (Rgemm
+// 'T', 'N') and solve (Rtrsm('L', 'U', 'T', 'N')).  nb <= 1 or nb >= n is Rpotrf2 on the
+// whole matrix (Rpotrf.cpp:86-91).  Kernels after a failed diagonal do nothing.
+static cudaError_t launch_ltx(bool upper, bool unit, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B,
+                              int ldb, const int *info, cudaStream_t st);
+
+static void potrf2_upper_plan(int n, size_t *ws)
+{
+    if (n <= POTRF2_CTA_MAX)
+        return;
+    const int n1 = n / 2, n2 = n - n1;
+    potrf2_upper_plan(n1, ws);
+    *ws = std::max(*ws, gemm_workspace_bytes(n2, n2, n1));
+    potrf2_upper_plan(n2, ws);
+}
+
+size_t rpotrf_upper_workspace_bytes(int n, int nb)
+{
+    size_t ws = 0;
+    if (nb <= 1 || nb >= n) {
+        potrf2_upper_plan(n, &ws);
+        return ws;
+    }
+    for (int j = 0; j < n; j += nb) {
+        const int jb = imin(nb, n - j);
+        if (j > 0) {
+            ws = std::max(ws, gemm_workspace_bytes(jb, jb, j));
+            if (j + jb < n)
+                ws = std::max(ws, gemm_workspace_bytes(jb, n - j - jb, j));
+        }
+        potrf2_upper_plan(jb, &ws);
+    }
+    return ws;
+}
+
+static cudaError_t potrf2_upper(uint32_t *A, int lda, int off, int n, int *info, void *ws, cudaStream_t st)
+{
+    const size_t L = (size_t)lda;
+    if (n <= POTRF2_CTA_MAX) {
+        potrf2_upper_cta_kernel<<<1, POTRF2_CTA_THREADS, 0, st>>>(A + off + (size_t)off * L, L, n, off, info);
+        return cudaGetLastError();
+    }
+    const int n1 = n / 2, n2 = n - n1;
+    cudaError_t e = potrf2_upper(A, lda, off, n1, info, ws, st);
+    if (e == cudaSuccess)
+        e = launch_ltx(true, false, n1, n2, A + off + (size_t)off * L, lda, A + off + (size_t)(off + n1) * L, lda,
+                       info, st);
+    if (e == cudaSuccess)
+        e = gemm_launch_tri(TRI_UPPER, false, true, n2, n2, n1, 0xC0000000u /* -1 */,
+                            A + off + (size_t)(off + n1) * L, lda, A + off + (size_t)(off + n1) * L, lda, P32_ONE,
+                            A + (off + n1) + (size_t)(off + n1) * L, lda, ws, st, info);
+    if (e == cudaSuccess)
+        e = potrf2_upper(A, lda, off + n1, n2, info, ws, st);
+    return e;
+}
+
+cudaError_t rpotrf_upper_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st)
+{
+    if (nb <= 1 || nb >= n)
+        return potrf2_upper(A, lda, 0, n, info, ws, st);
+    const size_t L = (size_t)lda;
+    for (int j = 0; j < n; j += nb) {
+        const int jb = imin(nb, n - j);
+        cudaError_t e = cudaSuccess;
+        if (j > 0) // Rsyrk('U', 'T', jb, j, -1, A(0:j, j:j+jb), 1, A(j:j+jb, j:j+jb))
+            e = gemm_launch_tri(TRI_UPPER, false, true, jb, jb, j, 0xC0000000u /* -1 */, A + (size_t)j * L, lda,
+                                A + (size_t)j * L, lda, P32_ONE, A + j + (size_t)j * L, lda, ws, st, info);
+        if (e == cudaSuccess)
+            e = potrf2_upper(A, lda, j, jb, info, ws, st);
+        if (e == cudaSuccess && j + jb < n) {
+            const int nr = n - j - jb;
+            if (j > 0) // Rgemm('T', 'N', jb, nr, j, -1, A(0:j, j:j+jb), A(0:j, j+jb:n), 1, A(j:j+jb, j+jb:n))
+                e = gemm_launch_tri(TRI_FULL, false, true, jb, nr, j, 0xC0000000u /* -1 */, A + (size_t)j * L, lda,
+                                    A + (size_t)(j + jb) * L, lda, P32_ONE, A + j + (size_t)(j + jb) * L, lda, ws, st,
+                                    info);
+            if (e == cudaSuccess) // Rtrsm('L', 'U', 'T', 'N', jb, nr, 1, A(j:j+jb, j:j+jb), A(j:j+jb, j+jb:n))
+                e = launch_ltx(true, false, jb, nr, A + j + (size_t)j * L, lda, A + j + (size_t)(j + jb) * L, lda,
+                               info, st);
+        }
+        if (e != cudaSuccess)
+            return e;
     }
     return cudaGetLastError();
 }
@@ -745,29 +1119,36 @@ cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int
     return e;
 }
 
-// Rpotrs.cpp:95-106 (uplo = 'L'): L forward, L^T backward.
-cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
+// The dot-form solves with the triangle transposed: L^-T B (Rtrsm('L', 'L', 'T'),
+// Rtrsm.cpp:175-186) or, with `upper`, U^-T B (Rtrsm('L', 'U', 'T'), Rtrsm.cpp:160-173).
+// One block per right-hand side: the scan-form kernel where its terms fit in shared
+// memory (FP64 where 20n bytes fit, patterns where 12n do), else one thread's chain.
+// A nonzero *info (when given) turns the solve into a no-op.
+static cudaError_t launch_ltx(bool upper, bool unit, int n, int nrhs, const uint32_t *A, int lda, uint32_t *B,
+                              int ldb, const int *info, cudaStream_t st)
 {
-    const int threads = 1024;
-    cudaError_t e = launch_lln(nrhs, threads, A, lda, B, ldb, n, false, nullptr, st);
-    if (e != cudaSuccess)
-        return e;
-    // terms in FP64 where 20n bytes fit, as patterns where 12n bytes do
+    cudaError_t e = cudaSuccess;
     const size_t pc8 = llt_pc_smem_bytes(n, sizeof(double)), pc4 = llt_pc_smem_bytes(n, sizeof(uint32_t));
     if (pc8 <= (size_t)LLT_SMEM_MAX || pc4 <= (size_t)LLT_SMEM_MAX) {
         const bool f64 = pc8 <= (size_t)LLT_SMEM_MAX;
         const size_t pc = f64 ? pc8 : pc4;
+        const void *fn = f64 ? (upper ? (const void *)trsm_llt_pc_kernel<double, true>
+                                      : (const void *)trsm_llt_pc_kernel<double, false>)
+                             : (upper ? (const void *)trsm_llt_pc_kernel<uint32_t, true>
+                                      : (const void *)trsm_llt_pc_kernel<uint32_t, false>);
         if (pc > 48 * 1024) {
-            e = f64 ? cudaFuncSetAttribute(trsm_llt_pc_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc)
-                    : cudaFuncSetAttribute(trsm_llt_pc_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)pc);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc);
             if (e != cudaSuccess)
                 return e;
         }
-        if (f64)
-            trsm_llt_pc_kernel<double><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
+        if (f64 && upper)
+            trsm_llt_pc_kernel<double, true><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+        else if (f64)
+            trsm_llt_pc_kernel<double, false><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+        else if (upper)
+            trsm_llt_pc_kernel<uint32_t, true><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         else
-            trsm_llt_pc_kernel<uint32_t><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, false, nullptr);
+            trsm_llt_pc_kernel<uint32_t, false><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         return cudaGetLastError();
     }
     const size_t col = (size_t)n * 4;
@@ -777,7 +1158,42 @@ cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uin
         if (e != cudaSuccess)
             return e;
     }
-    trsm_llt_kernel<<<nrhs, 32, staged ? col : 0, st>>>(A, lda, B, ldb, n, staged, false, nullptr);
+    trsm_llt_kernel<<<nrhs, 32, staged ? col : 0, st>>>(A, lda, B, ldb, n, staged, unit, upper, info);
+    return cudaGetLastError();
+}
+
+// Rpotrs.cpp:95-106 (uplo = 'L'): L forward, L^T backward.
+cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
+{
+    const int threads = 1024;
+    cudaError_t e = launch_lln(nrhs, threads, A, lda, B, ldb, n, false, nullptr, st);
+    if (e != cudaSuccess)
+        return e;
+    return launch_ltx(false, false, n, nrhs, A, lda, B, ldb, nullptr, st);
+}
+
+// Rpotrs.cpp:84-95 (uplo = 'U'): U^T forward (Rtrsm('L', 'U', 'T', 'N')), then U backward
+// (Rtrsm('L', 'U', 'N', 'N')).
+cudaError_t rpotrs_upper_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb, cudaStream_t st)
+{
+    cudaError_t e = launch_ltx(true, false, n, nrhs, A, lda, B, ldb, nullptr, st);
+    if (e != cudaSuccess)
+        return e;
+    return launch_lun(nrhs, 1024, A, lda, B, ldb, n, false, nullptr, st);
+}
+
+// Rgetrs.cpp:99-113 (trans = 'T' or 'C'): U^T forward (non-unit), L^T backward (unit),
+// then the interchanges applied in reverse order (Rlaswp with incx = -1).
+cudaError_t rgetrs_trans_launch(int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb,
+                                cudaStream_t st)
+{
+    cudaError_t e = launch_ltx(true, false, n, nrhs, A, lda, B, ldb, nullptr, st);
+    if (e != cudaSuccess)
+        return e;
+    e = launch_ltx(false, true, n, nrhs, A, lda, B, ldb, nullptr, st);
+    if (e != cudaSuccess)
+        return e;
+    laswp_kernel<<<(nrhs + 127) / 128, 128, 0, st>>>(B, ldb, nrhs, 1, n, ipiv, -1, nullptr);
     return cudaGetLastError();
 }
 

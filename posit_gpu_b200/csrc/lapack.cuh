@@ -18,5 +18,13 @@ cudaError_t rgetrs_launch(int n, int nrhs, const uint32_t *A, int lda, const int
                           cudaStream_t st);
 cudaError_t rpotrs_lower_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb,
                                 cudaStream_t st);
+// Upper Cholesky (nb-dependent bits: the caller's nb is the reference's), its solve, and
+// the transposed LU solve.
+size_t rpotrf_upper_workspace_bytes(int n, int nb);
+cudaError_t rpotrf_upper_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st);
+cudaError_t rpotrs_upper_launch(int n, int nrhs, const uint32_t *A, int lda, uint32_t *B, int ldb,
+                                cudaStream_t st);
+cudaError_t rgetrs_trans_launch(int n, int nrhs, const uint32_t *A, int lda, const int *ipiv, uint32_t *B, int ldb,
+                                cudaStream_t st);
 
 } // namespace pg

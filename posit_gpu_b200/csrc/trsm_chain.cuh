@@ -32,28 +32,33 @@ PG_HD dp32 chain_a(uint32_t l) { return decode_dz_bf(l == P32_NAR ? 0u : l); }
 
 // b (this thread's right-hand side, m entries; shared or global memory) is overwritten
 // with L^-T b.  L is read-only.  Host and device (the host build is what the CPU tests run).
-PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, int m, bool unit)
+// With `upper`, the triangle is an upper one, U, and b is overwritten with U^-T b
+// (Rtrsm('L', 'U', 'T'), Rtrsm.cpp:160-173): for i = 0 .. m-1, t = b_i, t = t - u_ki*b_k for
+// k = 0 .. i-1 (ascending), b_i = t / u_ii -- the same chain run forwards.
+PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, int m, bool unit, bool upper = false)
 {
     constexpr int U = CHAIN_BLOCK;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint32_t *li = L + (size_t)i * ldl; // column i of L: a_ki for k > i
+    for (int step = 0; step < m; ++step) {
+        const int i = upper ? step : m - 1 - step;
+        const uint32_t *li = L + (size_t)i * ldl; // column i: a_ki for k > i (lower) or k < i (upper)
         const uint32_t bi = b[i];                 // alpha*b with alpha == 1
         uint32_t nar = bi == P32_NAR;
         dp32 c = decode_dz(nar ? 0u : bi);
-        int k = i + 1;
-        if (k + U <= m) {
+        int k = upper ? 0 : i + 1;
+        const int kend = upper ? i : m;
+        if (k + U <= kend) {
             uint32_t lv[U], bv[U];
 #pragma unroll
             for (int j = 0; j < U; ++j) {
                 lv[j] = li[k + j];
                 bv[j] = b[k + j];
             }
-            for (; k + U <= m; k += U) {
-                // next block's operands (indexes clamped into [0, m))
+            for (; k + U <= kend; k += U) {
+                // next block's operands (indexes clamped into [0, kend))
                 uint32_t ln[U], bn[U];
 #pragma unroll
                 for (int j = 0; j < U; ++j) {
-                    const int kk = k + U + j < m ? k + U + j : m - 1;
+                    const int kk = k + U + j < kend ? k + U + j : kend - 1;
                     ln[j] = li[kk];
                     bn[j] = b[kk];
                 }
@@ -84,7 +89,7 @@ PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, in
                 }
             }
         }
-        for (; k < m; ++k) {
+        for (; k < kend; ++k) {
             const uint32_t l = li[k], bk = b[k];
             nar |= (l == P32_NAR) | (bk == P32_NAR);
             c = dmac_chain(c, chain_neg_b(bk), chain_a(l));
@@ -338,6 +343,28 @@ PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint3
     return r;
 }
 
+// The same step with the rounding done on the FP64 pattern.  Within one regime the posit
+// keeps fb fraction bits in every binade, so rounding the exact sum s to the posit grid is
+// rounding its FP64 significand to fb bits, to nearest, ties to even: add 2^(sh-1) - 1
+// plus the last kept bit to the pattern's magnitude and clear the sh = 52 - fb bits below
+// (a carry out of the significand moves into the exponent, which is the correct result).
+// On the dependent path that is one FP64 addition and a few integer operations instead of
+// an AND, an FP64 multiply and two FP64 additions.  sh <= 31: the kept bit and the cleared
+// bits are in the low word.
+PG_HD double f64_posit_add_reg_int(double t, double q, uint32_t sh, int32_t kreg, uint32_t &bad)
+{
+    const double s = f64_add(t, q);
+    const uint64_t sb = f64_bits(s);
+    const uint64_t rb = (sb + (((uint64_t)1 << (sh - 1)) - 1) + ((sb >> sh) & 1)) & ~(((uint64_t)1 << sh) - 1);
+    // off the dependent path
+    const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
+    const int32_t gap = et > eq ? et - eq : eq - et;
+    const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
+    const int32_t ks = ((int32_t)((sb >> 52) & 0x7FF) - 1023) >> 2;
+    bad |= (risky | (ks != kreg)) ? 0x40000000u : 0u;
+    return f64_from_bits(rb);
+}
+
 // t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-regime step: blocks of
 // CHAIN_BLOCK steps without a branch, a flagged block redone step by step exactly.
 // Terms read from FP64 values or from posit32 patterns (converted on load).
@@ -367,9 +394,17 @@ PG_HD double chain_add_run_reg(double t, Q q, int count)
             v[j] = q[k + j];
         const double t0 = t;
         uint32_t bad = in ? 0u : 0x40000000u;
+        const int32_t run = (kreg ^ (kreg >> 31)) + 1; // fb = 28 - run
+        if (run <= 7) {                                 // sh = 24 + run <= 31
+            const uint32_t sh = 24u + (uint32_t)run;
 #pragma unroll
-        for (int j = 0; j < U; ++j)
-            t = f64_posit_add_reg(t, v[j], G, kreg, bad);
+            for (int j = 0; j < U; ++j)
+                t = f64_posit_add_reg_int(t, v[j], sh, kreg, bad);
+        } else {
+#pragma unroll
+            for (int j = 0; j < U; ++j)
+                t = f64_posit_add_reg(t, v[j], G, kreg, bad);
+        }
         if (bad & 0x40000000u) { // (from q: a dynamic index into v would put v in local memory)
             t = t0;
             for (int j = 0; j < U; ++j)

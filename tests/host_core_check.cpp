@@ -56,6 +56,11 @@ void hc_dmac_chain_n(const uint32_t *c, const uint32_t *t, const uint32_t *a, ui
 }
 // one right-hand side of the L^T solve: trsm_chain.cuh's llt_chain, built for the host
 void hc_llt_solve(const uint32_t *L, long ld, uint32_t *b, int m) { llt_chain(L, (size_t)ld, b, m, false); }
+// the same chain run forwards on an upper triangle: U^T solve (Rgetrs 'T', Rpotrs 'U')
+void hc_utt_solve(const uint32_t *U, long ld, uint32_t *b, int m, int unit)
+{
+    llt_chain(U, (size_t)ld, b, m, unit != 0, true);
+}
 // decode_dz_bf against decode_dz on n patterns (NaR skipped); returns mismatches
 long hc_decode_bf_mismatch(const uint32_t *u, long n)
 {

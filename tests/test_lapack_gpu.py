@@ -21,8 +21,11 @@ def _spd(rng, n):
 
 
 @pytest.mark.parametrize("m,n,nb", [(1, 1, 256), (5, 5, 2), (37, 37, 8), (100, 100, 32), (300, 300, 64),
-                                    (257, 257, 256), (700, 700, 256), (90, 60, 16), (60, 90, 16)])
+                                    (257, 257, 256), (700, 700, 256), (90, 60, 16), (60, 90, 16),
+                                    (5000, 130, 64), (4100, 600, 512), (4500, 300, 600)])
 def test_rgetrf_bit_exact(cuda_ok, m, n, nb):
+    """Panels up to 4096 rows (and 512 columns) run in one thread block, taller or wider
+    ones as two launches per column; both are covered."""
     import posit_gpu_b200 as pg
     rng = np.random.default_rng(m * 1000 + n)
     A = _ge(rng, m, n)
@@ -66,7 +69,8 @@ def test_rgetrs_bit_exact(cuda_ok, n, nrhs):
     assert np.array_equal(g, o)
 
 
-@pytest.mark.parametrize("n,nb", [(1, 256), (5, 2), (64, 16), (300, 64), (520, 256), (700, 128)])
+@pytest.mark.parametrize("n,nb", [(1, 256), (5, 2), (64, 16), (300, 64), (520, 256), (700, 128), (900, 600),
+                                  (4300, 256)])
 def test_rpotrf_lower_bit_exact(cuda_ok, n, nb):
     import posit_gpu_b200 as pg
     rng = np.random.default_rng(n * 3 + nb)
@@ -151,10 +155,14 @@ def test_lapack_matches_reference_golden(cuda_ok):
         assert np.array_equal(xs, g[f"xs{i}"])
 
 
-def test_unsupported_variants_are_refused(cuda_ok):
+def test_bad_variant_letters_are_refused(cuda_ok):
+    """uplo / trans outside the reference's letters return the info code of argument 1
+    (Rpotrf.cpp:64-72, Rgetrs.cpp:60-71)."""
     import posit_gpu_b200 as pg
     S = np.zeros(4, np.uint32)
-    with pytest.raises(pg.PositError):
-        pg.Rpotrf("U", 2, S, 2)
     with pytest.raises(ValueError):
         pg.Rpotrf("X", 2, S, 2)
+    with pytest.raises(ValueError):
+        pg.Rpotrs("X", 2, 1, S, 2, S.copy(), 2)
+    with pytest.raises(ValueError):
+        pg.Rgetrs("X", 2, 1, S, 2, np.ones(2, np.int32), S.copy(), 2)

@@ -32,6 +32,7 @@ def hc(tmp_path_factory):
     lib.hc_chain.argtypes = [U32, U32, U32, U32, ctypes.c_long, ctypes.c_long]
     lib.hc_dmac_chain_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
     lib.hc_llt_solve.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
+    lib.hc_utt_solve.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int, ctypes.c_int]
     lib.hc_llt_solve_split.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int]
     lib.hc_llt_solve_scan.argtypes = [U32, ctypes.c_long, U32, ctypes.c_int, ctypes.c_int, I64]
     lib.hc_scan_row_check.argtypes = [ctypes.c_uint32, U32, ctypes.c_int, ctypes.c_int, I64]
@@ -165,6 +166,28 @@ def test_lower_transposed_solve_matches_oracle(hc):
             got = b.copy()
             hc.hc_llt_solve_scan(L, m, got, m, E, np.zeros(2, np.int64))
             assert np.array_equal(got, want), (m, kind, "scan", E)
+
+
+def test_upper_transposed_solve_matches_oracle(hc):
+    """The same chain run forwards on an upper triangle (trsm_chain.cuh's llt_chain with
+    upper = true) against the oracle's Rtrsm('L', 'U', 'T', 'N' / 'U'), Rtrsm.cpp:160-173."""
+    rng = np.random.default_rng(16)
+    for m, kind in ((1, "u"), (9, "u"), (120, "u"), (64, "w"), (50, "nar")):
+        U = oracle.from_double(rng.uniform(-1, 1, m * m))
+        if kind == "w":
+            U = oracle.from_double(np.sign(rng.uniform(-1, 1, m * m)) * 10.0 ** rng.uniform(-20, 20, m * m))
+        for i in range(m):
+            U[i + i * m] = oracle.p32(1.0 + rng.uniform(0, 1))
+        b = oracle.from_double(rng.uniform(-1, 1, m))
+        b[::5] = 0
+        if kind == "nar":
+            U[2 + (m - 1) * m] = oracle.P32_NAR
+        for diag, unit in ((b"N", 0), (b"U", 1)):
+            want = b.copy()
+            oracle.orc.orc_rtrsm(b"L", b"U", b"T", diag, m, 1, oracle.P32_ONE, U, m, want, m)
+            got = b.copy()
+            hc.hc_utt_solve(U, m, got, m, unit)
+            assert np.array_equal(got, want), (m, kind, diag)
 
 
 def test_branch_free_decode_matches_decode(hc):
