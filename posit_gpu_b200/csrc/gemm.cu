@@ -16,13 +16,15 @@
 //     [m-tile][k-tile][l][i], B as [n-tile][k-tile][l][j], plus a NaR flag per row and
 //     column.  Transposition is absorbed here, so the main kernel never sees lda/ldb.
 //  2. main kernel: one CTA per 64x32 tile of C, 256 threads, 4x2 outputs per thread held
-//     in FP64 across the whole k loop, 4 CTAs per SM.  Each 16-deep k tile of A and B
+//     in FP64 across the whole k loop (two sets taking turns, gemm_tile.cuh), 3 CTAs per
+//     SM.  Each 16-deep k tile of A and B
 //     (8 KB + 4 KB) is brought into shared memory by the bulk-copy (TMA) engine
 //     (cp.async.bulk + mbarrier transaction counts, 3 stages, every wait bounded).  The
 //     inner step is the FP64 form of p32_mul + p32_add (posit32.cuh, f64_posit_mac) with
-//     the rounding constants in a shared-memory table, committed branch-free; the rare
-//     step it flags (an inexact FP64 sum, a result outside the fast window) is redone
-//     exactly, in order, right after its k step.
+//     the rounding constants in a shared-memory table, written into the other accumulator
+//     set without a select; the rare step it flags (an inexact FP64 sum, a result outside
+//     the fast window) is redone exactly from the set it read, in order, right after its
+//     k step.
 #include "gemm.cuh"
 #include "gemm_tile.cuh"
 #include "posit32.cuh"

@@ -15,7 +15,7 @@ constexpr int BN = 16 * TN;
 constexpr int BK = 16;
 constexpr int NTHREADS = 256;
 constexpr int STAGES = 3;
-constexpr int MIN_CTAS_PER_SM = 4;
+constexpr int MIN_CTAS_PER_SM = 3;
 static_assert(TM % 2 == 0 && TN % 2 == 0, "operands are loaded in pairs");
 
 // Which entries of C a launch writes (gemm_launch_tri).
