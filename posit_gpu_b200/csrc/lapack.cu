@@ -26,6 +26,7 @@
 #include "lapack.cuh"
 
 #include <algorithm>
+#include <cooperative_groups.h>
 #include "posit32.cuh"
 #include "trsm_chain.cuh"
 
@@ -186,73 +187,118 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
 }
 
 // ---------------------------------------------------------------------------
-// LU panel in one CTA (panels of at most PANEL1_MAX_M rows): the same per-column steps as
-// lu_pivot_kernel + lu_update_kernel -- iRamax with first-max tie-break, the interchange
-// across the panel, the scaling decision, the scaled column, the rank-1 update in the FP64
-// step -- in the same per-element order, with a barrier between steps instead of a kernel
-// boundary, so a whole panel is one launch.  For short panels the two launches per column
-// (a few microseconds each) cost more than the arithmetic; for tall ones the
-// many-block update wins, so the host picks by the panel height.
+// LU panel in one thread-block cluster: the per-column steps of lu_pivot_kernel +
+// lu_update_kernel -- iRamax with first-max tie-break, the interchange across the panel,
+// the scaling decision, the scaled column, the rank-1 update in the FP64 step -- in the
+// same per-element order, one launch per panel.  Up to 8 CTAs of 1024 threads (8 SMs);
+// row i of the panel belongs to thread i mod (CTAs * 1024) for the whole panel, so a thread
+// reads back only what it wrote itself, except:
+//   * the pivot candidates: each CTA's best (key, row) goes to its shared memory and every
+//     CTA reads all of them through distributed shared memory after a cluster barrier,
+//     then decides the pivot itself (the same bits everywhere);
+//   * the interchange of rows k and p, done by CTA 0 and followed by a second cluster
+//     barrier before anyone reads row k (the -u_kc) or its own rows again.
+// The cluster barriers are the hardware's (barrier.cluster, release/acquire at cluster
+// scope, all CTAs of a cluster co-scheduled).  Data another SM may have written is read
+// with ld.global.cg (L2, never a stale L1 line).  A panel too tall or too wide for this
+// to beat the many-block update runs the two-launch form instead (host side).
 // ---------------------------------------------------------------------------
 constexpr int PANEL1_THREADS = 1024;
 constexpr int PANEL1_MAX_JB = 512;
-constexpr int PANEL1_MAX_M = 4096;
+constexpr int PANEL1_MAX_CTAS = 8;
 
-__global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cta_kernel(uint32_t *__restrict__ P, size_t lda, int M,
-                                                                      int jb, int row0, int *__restrict__ ipiv,
-                                                                      int *__restrict__ info)
+__device__ __forceinline__ uint32_t ldcg(const uint32_t *p) { return __ldcg(p); }
+__device__ __forceinline__ void stcg(uint32_t *p, uint32_t v) { __stcg(p, v); }
+
+// Row i of the panel is thread (i mod G)'s; its first row at or after `from`.
+__device__ __forceinline__ int first_owned(int g, int G, int from) { return from + ((g - from % G) + G) % G; }
+
+__global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
+                                                                          int M, int jb, int row0,
+                                                                          int *__restrict__ ipiv,
+                                                                          int *__restrict__ info)
 {
+    namespace cgs = cooperative_groups;
+    cgs::cluster_group cluster = cgs::this_cluster();
+    const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
     __shared__ int32_t s_key[32];
     __shared__ int s_idx[32];
+    __shared__ int32_t s_ckey; // this CTA's pivot candidate, read by the whole cluster:
+    __shared__ int s_cidx;     // key, row and the row's value (CTA 0's interchange may
+    __shared__ uint32_t s_cval; // overwrite the row in global memory meanwhile)
     __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row, FP64
     __shared__ PivotInfo s_pi;
-    if (*info < 0)
+    if (*info < 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
     for (int k = 0; k < jb; ++k) {
         const uint32_t *col = P + (size_t)k * lda;
-        // iRamax over rows [k, M) (iRamax.cpp:65-71), as in lu_pivot_kernel
+        // this thread's rows of [k, M): iRamax order (iRamax.cpp:65-71), first max wins
         int32_t best = INT32_MIN;
         int bidx = -1;
-        for (int i = k + tid; i < M; i += PANEL1_THREADS) {
-            const int32_t key = (int32_t)pabs(col[i]);
+        uint32_t bval = 0;
+        for (int i = first_owned(g, G, k); i < M; i += G) {
+            const uint32_t v = ldcg(col + i);
+            const int32_t key = (int32_t)pabs(v);
             if (bidx < 0 || key > best) {
                 best = key;
                 bidx = i;
+                bval = v;
             }
         }
+        __shared__ uint32_t s_val[32];
 #pragma unroll
         for (int round = 0; round < 2; ++round) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
                 const int32_t k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
                 const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
+                const uint32_t v2 = __shfl_down_sync(0xFFFFFFFFu, bval, off);
                 if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
                     best = k2;
                     bidx = i2;
+                    bval = v2;
                 }
             }
             if (round == 0) {
                 if (lane == 0) {
                     s_key[warp] = best;
                     s_idx[warp] = bidx;
+                    s_val[warp] = bval;
                 }
                 __syncthreads();
                 best = s_key[lane];
                 bidx = s_idx[lane];
+                bval = s_val[lane];
             }
         }
         if (tid == 0) {
-            const int p = bidx;
-            const uint32_t piv = col[p];
-            ipiv[row0 + k] = row0 + p + 1; // 1-based, global
+            s_ckey = best;
+            s_cidx = bidx;
+            s_cval = bval;
+        }
+        cluster.sync(); // candidates visible; every row of column k is final
+        if (tid == 0) {
+            int p = -1;
+            int32_t pk = INT32_MIN;
+            uint32_t piv = 0;
+            for (int r = 0; r < ncta; ++r) {
+                const int32_t k2 = *cluster.map_shared_rank(&s_ckey, r);
+                const int i2 = *cluster.map_shared_rank(&s_cidx, r);
+                if (i2 >= 0 && (p < 0 || k2 > pk || (k2 == pk && i2 < p))) {
+                    pk = k2;
+                    p = i2;
+                    piv = *cluster.map_shared_rank(&s_cval, r);
+                }
+            }
             PivotInfo pi;
             pi.row = p;
             pi.piv = piv;
             if (piv == 0) {
                 pi.mode = 0;
                 pi.recip = 0;
-                if (*info == 0)
+                if (rank == 0 && *info == 0)
                     *info = row0 + k + 1;
             } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
                 pi.mode = 1;
@@ -261,33 +307,34 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cta_kernel(uint32_t *
                 pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
                 pi.recip = 0;
             }
+            if (rank == 0)
+                ipiv[row0 + k] = row0 + p + 1; // 1-based, global
             s_pi = pi;
         }
         __syncthreads();
         const PivotInfo pi = s_pi;
-        if (pi.piv != 0 && pi.row != k) { // interchange rows k and p across the panel (Rgetrf2.cpp:107-117)
+        if (rank == 0 && pi.piv != 0 && pi.row != k) { // Rgetrf2.cpp:107-117
             for (int c = tid; c < jb; c += PANEL1_THREADS) {
                 uint32_t *pc = P + (size_t)c * lda;
-                const uint32_t t = pc[k];
-                pc[k] = pc[pi.row];
-                pc[pi.row] = t;
+                const uint32_t t = ldcg(pc + k);
+                stcg(pc + k, ldcg(pc + pi.row));
+                stcg(pc + pi.row, t);
             }
         }
-        __syncthreads();
+        cluster.sync(); // the interchange is visible
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_u[c] = -p32_to_double(P[k + (size_t)c * lda]);
+            s_u[c] = -p32_to_double(ldcg(P + k + (size_t)c * lda));
         __syncthreads();
-        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS) {
+        for (int i = first_owned(g, G, k + 1); i < M; i += G) {
             uint32_t *pik = P + i + (size_t)k * lda;
-            const uint32_t l = lu_scaled(*pik, pi);
-            *pik = l;
+            const uint32_t l = lu_scaled(ldcg(pik), pi);
+            stcg(pik, l);
             const double dl = p32_to_double(l);
             for (int c = k + 1; c < jb; ++c) { // a_ic + (-u_kc)*l_i in the FP64 step
                 uint32_t *pc = P + i + (size_t)c * lda;
-                *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_u[c], dl));
+                stcg(pc, p32_from_double_exact(f64_posit_mac_checked(p32_to_double(ldcg(pc)), s_u[c], dl)));
             }
         }
-        __syncthreads();
     }
 }
 
@@ -749,52 +796,61 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
     }
 }
 
-// Lower Cholesky panel in one CTA, the counterpart of chol_diag_kernel +
-// chol_update_kernel: per column the square root and reciprocal of the diagonal
-// (Rpotrf2.cpp:90-97), the column below it times the reciprocal (Rtrsm.cpp:265-268), the
-// rank-1 update of the lower part of the rest of the panel, with barriers in between.
-__global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cta_kernel(uint32_t *__restrict__ P, size_t lda,
-                                                                        int M, int jb, int row0,
-                                                                        int *__restrict__ info)
+// Lower Cholesky panel in one thread-block cluster, the counterpart of chol_diag_kernel +
+// chol_update_kernel, with the same row ownership and reads as lu_panel_cluster_kernel: per
+// column a cluster barrier, every CTA reads the final a_kk and takes its square root and
+// reciprocal (Rpotrf2.cpp:90-97; the same bits everywhere), each thread scales its rows
+// below the diagonal (Rtrsm.cpp:265-268), a cluster barrier, CTA 0 stores l_kk (no CTA
+// reads a_kk after that barrier), the -l_ck of the panel rows into shared memory, the
+// rank-1 update of each thread's rows.
+__global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
+                                                                            int M, int jb, int row0,
+                                                                            int *__restrict__ info)
 {
+    namespace cgs = cooperative_groups;
+    cgs::cluster_group cluster = cgs::this_cluster();
+    const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
     __shared__ double s_l[PANEL1_MAX_JB]; // -l_ck of the current column, FP64
-    __shared__ uint32_t s_recip;
+    __shared__ uint32_t s_recip, s_lkk;
     __shared__ int s_stop;
-    if (*info != 0)
+    if (*info != 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x;
+    const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
     for (int k = 0; k < jb; ++k) {
         uint32_t *pk = P + (size_t)k * lda;
+        cluster.sync(); // every update of column k is done
         if (tid == 0) {
-            const uint32_t akk = pk[k];
+            const uint32_t akk = ldcg(pk + k);
             s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
             if (s_stop) {
-                *info = row0 + k + 1;
+                if (rank == 0)
+                    *info = row0 + k + 1;
             } else {
-                const uint32_t lkk = psqrt(akk);
-                s_recip = pdiv(P32_ONE, lkk);
-                pk[k] = lkk;
+                s_lkk = psqrt(akk);
+                s_recip = pdiv(P32_ONE, s_lkk);
             }
         }
         __syncthreads();
-        if (s_stop)
+        if (s_stop) // decided from the same a_kk in every CTA
             return;
         const uint32_t recip = s_recip;
-        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS)
-            pk[i] = pmul(recip, pk[i]);
-        __syncthreads();
+        for (int i = first_owned(g, G, k + 1); i < M; i += G)
+            stcg(pk + i, pmul(recip, ldcg(pk + i)));
+        cluster.sync(); // the scaled column is visible, and every CTA has read a_kk
+        if (rank == 0 && tid == 0)
+            stcg(pk + k, s_lkk);
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_l[c] = -p32_to_double(pk[c]);
+            s_l[c] = -p32_to_double(ldcg(pk + c));
         __syncthreads();
-        for (int i = k + 1 + tid; i < M; i += PANEL1_THREADS) {
-            const double dl = p32_to_double(pk[i]);
+        for (int i = first_owned(g, G, k + 1); i < M; i += G) {
+            const double dl = p32_to_double(ldcg(pk + i));
             const int cend = min(jb - 1, i);
             for (int c = k + 1; c <= cend; ++c) { // a_ic + (-l_ck)*l_i in the FP64 step
                 uint32_t *pc = P + i + (size_t)c * lda;
-                *pc = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(*pc), s_l[c], dl));
+                stcg(pc, p32_from_double_exact(f64_posit_mac_checked(p32_to_double(ldcg(pc)), s_l[c], dl)));
             }
         }
-        __syncthreads();
     }
 }
 
@@ -922,6 +978,36 @@ size_t rgetrf_workspace_bytes(int m, int n, int nb)
     return panel_ws_bytes(m) + g;
 }
 
+// The panel form: CTAs of a cluster panel (1..8, one per 1024 rows), or 0 for the
+// two-launch form.  A cluster panel's column costs two cluster barriers plus the rank-1
+// update of its rows on at most 8 SMs; the two-launch form costs two dependent launches
+// (about 7 microseconds each) with the update spread over all SMs.  The crossover, about
+// 1.5e-5 microseconds per panel entry against 12 microseconds, is at M*jb ~ 8e5.
+static int panel_cluster_ctas(int M, int jb)
+{
+    if (jb > PANEL1_MAX_JB || (long long)M * jb > 800000LL)
+        return 0;
+    return std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_THREADS - 1) / PANEL1_THREADS));
+}
+
+template <class... Args>
+static cudaError_t launch_panel_cluster(void (*kernel)(Args...), int ncta, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ncta);
+    cfg.blockDim = dim3(PANEL1_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)ncta;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 static dim3 panel_grid(int M, int jb, int k)
 {
     return dim3((unsigned)imax((M - k - 1 + PANEL_ROWS - 1) / PANEL_ROWS, 1),
@@ -945,8 +1031,11 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         const int M = m - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j; // indexed by panel-local row
-        if (M <= PANEL1_MAX_M && jb <= PANEL1_MAX_JB) {
-            lu_panel_cta_kernel<<<1, PANEL1_THREADS, 0, st>>>(P, L, M, jb, j, ipiv, info);
+        const int ncta = panel_cluster_ctas(M, jb);
+        if (ncta > 0) {
+            cudaError_t e = launch_panel_cluster(lu_panel_cluster_kernel, ncta, st, P, L, M, jb, j, ipiv, info);
+            if (e != cudaSuccess)
+                return e;
         } else {
             lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, 0, j, ipiv, info, pinfo, lc, -1);
             for (int k = 0; k < jb; ++k) {
@@ -998,8 +1087,11 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         const int M = n - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j;
-        if (M <= PANEL1_MAX_M && jb <= PANEL1_MAX_JB) {
-            chol_panel_cta_kernel<<<1, PANEL1_THREADS, 0, st>>>(P, L, M, jb, j, info);
+        const int ncta = panel_cluster_ctas(M, jb);
+        if (ncta > 0) {
+            cudaError_t e = launch_panel_cluster(chol_panel_cluster_kernel, ncta, st, P, L, M, jb, j, info);
+            if (e != cudaSuccess)
+                return e;
         } else {
             chol_diag_kernel<<<1, 256, 0, st>>>(P, L, M, jb, 0, j, info, sync, lc, -1);
             for (int k = 0; k < jb; ++k) {
