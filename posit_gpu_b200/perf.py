@@ -19,16 +19,16 @@ SM_MAX_MHZ = 1965.0
 
 # Warp instructions issued by gemm_main_kernel per posit multiply-add:
 # smsp__inst_executed.sum / (m*n*k) for one NN launch at m = n = k = 4096
-# (57,507,661,291 / 68,719,476,736 = 0.8368, i.e. 26.78 thread instructions).  Of
-# those, 11 per multiply-add run on the FP64 pipe (DMUL, DFMA, 7 DADD, 2 DSETP): FP64 pipe
-# 58.1 %, ALU pipe 44.5 %, issue 71.1 % busy in the same capture.
-WARP_INST_PER_MAD = 0.8368
+# (50,306,712,730 / 68,719,476,736 = 0.7321, i.e. 23.43 thread instructions).  Of those,
+# 11 per multiply-add run on the FP64 pipe (DMUL, DFMA, 7 DADD, 2 DSETP): FP64 pipe
+# 66.0 %, ALU pipe 28.5 %, LSU 29.4 %, issue 70.7 % busy in the same capture.
+WARP_INST_PER_MAD = 0.7321
 FP64_WARP_INST_PER_MAD = 11 / 32
-INST_SOURCE = ("ncu --set full, gemm_main_kernel<false,false>, NN 4096^3 U[-1,1] "
+INST_SOURCE = ("ncu --set full, gemm_main_kernel<0,0>, NN 4096^3 U[-1,1] "
                "(profiles/gemm_main_kernel_nn_4096.md)")
 # DRAM bytes (read + write) per posit multiply-add of the same launch:
-# (7,385,502,000 + 71,760,128) / 68,719,476,736.
-MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1085
+# (7,468,817,000 + 72,625,152) / 68,719,476,736.
+MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1097
 
 
 def issue_peak_warp_inst_per_s(sm_mhz):
@@ -45,7 +45,7 @@ def fp64_pipe_peak_warp_inst_per_s(sm_mhz):
 # the script that compiles them (flags included); the benchmark recomputes the digest and,
 # when it differs, marks the count stale and reports no roofline fraction from it.
 KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh", "build.py"]
-INST_SOURCE_DIGEST = None
+INST_SOURCE_DIGEST = "dc10a8365209bb53992d6ac760cc868b8276bb1b8d3380037f399a616ddbd161"
 
 
 def kernel_source_digest():
@@ -66,8 +66,9 @@ def inst_count_current():
 # m = n = 8192 - b, k = b (key b), from ncu dram__bytes_read.sum + dram__bytes_write.sum
 # of that launch.  Empty until measured; the benchmark then reports no traffic figure for
 # the shape rather than one scaled from another shape.
-TRAILING_TRAFFIC_BYTES = {}
-TRAILING_TRAFFIC_SOURCE = None
+TRAILING_TRAFFIC_BYTES = {16: 482229760, 32: 482424576, 64: 482440960, 128: 483245056, 256: 483035136}
+TRAILING_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, gemm_main_kernel<0,0>, "
+                           "one launch per shape (profiles/gemm_main_kernel_lu_trailing.md)")
 
 
 def trailing_traffic(k):
