@@ -772,7 +772,7 @@ def serve_arm(args):
         if m not in factors:
             F = fac_src[m]
             ipiv = np.zeros(n, np.int32)
-            info = pg.Rgetrf(n, n, F, n, ipiv, nb=64) if kind == 0 else pg.Rpotrf("L", n, F, n, nb=64)
+            info = pg.Rgetrf(n, n, F, n, ipiv) if kind == 0 else pg.Rpotrf("L", n, F, n)
             factors[m] = (F, ipiv, info)
         F, ipiv, info = factors[m]
         if kind == 0:

@@ -87,7 +87,8 @@ size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
  * the reference does, and its factors stay bit-identical; a Cholesky factorization that
  * stops (info > 0) leaves the not-yet-factored part of A in an unspecified state (the
  * reference's left-looking blocking and this right-looking one differ there).
- * nb <= 0 selects 256.  Upper Cholesky is the exception: in the reference's order
+ * nb <= 0 selects the panel width measured fastest on B200 for that n (the autotuner's
+ * table, built in).  Upper Cholesky is the exception: in the reference's order
  * (left-looking, each entry's update a dot product over the rows above it, Rpotrf.cpp:96-118)
  * its bits depend on nb, which is therefore the caller's -- the reference CPU routine's
  * own block size comes from iMlaenv, 64 (iMlaenv.cpp:223-228), and nb <= 0 selects that.
@@ -196,7 +197,7 @@ typedef struct {
     int lanes;            /* CUDA streams work units run on; 0 = 64 */
     int launch_threads;   /* threads issuing the units' CUDA work; 0 = 8 */
     int batch_max_n;      /* n <= this goes to the batched kernel; 0 = 256 (max POSIT_BATCH_MAX_N) */
-    int nb;               /* panel width of the blocked path; 0 = 64 */
+    int nb;               /* panel width of the blocked path; 0 = the tuned width for each n */
     int cache_off;        /* 1: never keep factors */
     int batch_lanes;      /* lanes reserved for batched units; 0 = 4 */
 } posit_server_config;

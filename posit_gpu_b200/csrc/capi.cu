@@ -208,7 +208,7 @@ int posit_rgemm(char transa, char transb, int m, int n, int k, uint32_t alpha, c
 }
 
 // ---- factorizations -------------------------------------------------------------
-static int pick_nb(int nb) { return nb > 0 ? nb : 256; }
+static int pick_nb(int nb, bool lu, int n) { return nb > 0 ? nb : pg::tuned_panel_width(lu, n); }
 static cudaStream_t as_stream(void *stream) { return stream ? (cudaStream_t)stream : cudaStreamPerThread; }
 
 int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream)
@@ -226,7 +226,7 @@ int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int 
     PG_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
     if (m == 0 || n == 0)
         return 0;
-    nb = pick_nb(nb);
+    nb = pick_nb(nb, true, m < n ? m : n);
     void *ws = nullptr;
     PG_TRY(cudaMallocAsync(&ws, pg::rgetrf_workspace_bytes(m, n, nb), st));
     cudaError_t e = pg::rgetrf_launch(m, n, A, lda, ipiv, nb, info, ws, st);
@@ -277,7 +277,7 @@ int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, 
     if (n == 0)
         return 0;
     // the upper factor depends on nb: the default is the reference's own block size
-    nb = upper ? (nb > 0 ? nb : POSIT_RPOTRF_UPPER_DEFAULT_NB) : pick_nb(nb);
+    nb = upper ? (nb > 0 ? nb : POSIT_RPOTRF_UPPER_DEFAULT_NB) : pick_nb(nb, false, n);
     const size_t wsb = upper ? pg::rpotrf_upper_workspace_bytes(n, nb) : pg::rpotrf_workspace_bytes(n, nb);
     void *ws = nullptr;
     if (wsb)

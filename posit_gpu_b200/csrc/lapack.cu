@@ -968,6 +968,23 @@ __global__ void __launch_bounds__(POTRF2_CTA_THREADS) potrf2_upper_cta_kernel(ui
 static int imin(int a, int b) { return a < b ? a : b; }
 static int imax(int a, int b) { return a > b ? a : b; }
 
+// Panel width for an n x n factorization when the caller passes nb <= 0: the widths the
+// autotuner (posit_gpu_b200/autotune.py) measured fastest on B200, by size bucket.  LU and
+// lower Cholesky give the same bits at every width.
+int tuned_panel_width(bool lu, int n)
+{
+    struct Row {
+        int n, lu, chol;
+    };
+    static const Row rows[] = {{0, 16, 16}, {512, 16, 16}, {1024, 16, 16}, {2048, 16, 16}, {4096, 16, 16},
+                               {8192, 16, 16}};
+    int nb = 16;
+    for (const Row &r : rows)
+        if (n >= r.n)
+            nb = lu ? r.lu : r.chol;
+    return nb;
+}
+
 size_t rgetrf_workspace_bytes(int m, int n, int nb)
 {
     int mn = imin(m, n);

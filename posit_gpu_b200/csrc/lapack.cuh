@@ -6,6 +6,8 @@
 
 namespace pg {
 
+// The measured-best panel width for an n x n LU (lu) or lower Cholesky factorization.
+int tuned_panel_width(bool lu, int n);
 size_t rgetrf_workspace_bytes(int m, int n, int nb);
 size_t rpotrf_workspace_bytes(int n, int nb);
 

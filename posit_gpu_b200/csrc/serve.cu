@@ -149,9 +149,16 @@ struct posit_server {
 
 namespace {
 
+// Panel width of a blocked unit: the configured one, or the tuned width for its n.
+int serve_nb(const posit_server *s, int kind, int n)
+{
+    return s->nb > 0 ? s->nb : pg::tuned_panel_width(kind == POSIT_BATCH_LU, n);
+}
+
 size_t ws_bytes(const posit_server *s, int kind, int n)
 {
-    return kind == POSIT_BATCH_LU ? pg::rgetrf_workspace_bytes(n, n, s->nb) : pg::rpotrf_workspace_bytes(n, s->nb);
+    const int nb = serve_nb(s, kind, n);
+    return kind == POSIT_BATCH_LU ? pg::rgetrf_workspace_bytes(n, n, nb) : pg::rpotrf_workspace_bytes(n, nb);
 }
 
 // Largest device footprint a request can have.
@@ -362,8 +369,8 @@ int launch_blocked(posit_server *s, Unit *u)
         void *ws = nullptr;
         SV_TRY(cudaMallocFromPoolAsync(&ws, ws_bytes(s, r.q.kind, n), s->pool, st));
         cudaError_t e = r.q.kind == POSIT_BATCH_LU
-                            ? pg::rgetrf_launch(n, n, f->dA, n, f->dipiv, s->nb, f->dinfo, ws, st)
-                            : pg::rpotrf_lower_launch(n, f->dA, n, s->nb, f->dinfo, ws, st);
+                            ? pg::rgetrf_launch(n, n, f->dA, n, f->dipiv, serve_nb(s, r.q.kind, n), f->dinfo, ws, st)
+                            : pg::rpotrf_lower_launch(n, f->dA, n, serve_nb(s, r.q.kind, n), f->dinfo, ws, st);
         cudaFreeAsync(ws, st);
         if (e != cudaSuccess)
             return fail_code(e);
@@ -710,7 +717,7 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
     s->max_inflight = c.max_inflight > 0 ? c.max_inflight : 4096;
     s->max_queue = c.max_queue > 0 ? c.max_queue : (1 << 20);
     s->batch_max_n = c.batch_max_n > 0 ? std::min(c.batch_max_n, POSIT_BATCH_MAX_N) : 256;
-    s->nb = c.nb > 0 ? c.nb : 64;
+    s->nb = c.nb > 0 ? c.nb : 0; // 0: the tuned width for each request's n
     s->cache_on = c.cache_off == 0;
     const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 64);
     const int nbatch = std::min(nlanes - 1, c.batch_lanes > 0 ? c.batch_lanes : 4);
