@@ -24,7 +24,7 @@ constexpr int BG_MAXB = 64; // largest tile side
 
 template <int TM_, int TN_>
 __device__ void batch_tile(const BatchGemmDesc &P, int mt, int nt, double *As, double *Ts, unsigned char *rnar,
-                           unsigned char *cnar, const uint32_t *ctab)
+                           unsigned char *cnar, const double *ctab)
 {
     constexpr int BM_ = 16 * TM_, BN_ = 16 * TN_;
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
@@ -140,14 +140,14 @@ __global__ void __launch_bounds__(BG_THREADS, 2)
                       int *__restrict__ next)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t *ctab = reinterpret_cast<uint32_t *>(smem); // rounding constants (F64ConstTable)
-    double *As = reinterpret_cast<double *>(smem + (size_t)F64_CONST_ENTRIES * sizeof(uint32_t));
+    double *ctab = reinterpret_cast<double *>(smem); // rounding constants (F64ConstTable8)
+    double *As = reinterpret_cast<double *>(smem + (size_t)F64_CONST_ENTRIES * sizeof(double));
     double *Ts = As + BK * BG_MAXB;
     unsigned char *rnar = reinterpret_cast<unsigned char *>(Ts + BK * BG_MAXB);
     unsigned char *cnar = rnar + BG_MAXB;
     __shared__ int s_item;
     for (int i = threadIdx.x; i < F64_CONST_ENTRIES; i += BG_THREADS)
-        ctab[i] = f64_round_const_top(i);
+        ctab[i] = f64_from_hi(f64_round_const_top(i));
     __syncthreads();
     for (;;) {
         if (threadIdx.x == 0)
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(BG_THREADS, 2)
 
 size_t batch_gemm_smem_bytes()
 {
-    return (size_t)F64_CONST_ENTRIES * sizeof(uint32_t) + 2 * (size_t)BK * BG_MAXB * sizeof(double) + 2 * BG_MAXB;
+    return (size_t)F64_CONST_ENTRIES * sizeof(double) + 2 * (size_t)BK * BG_MAXB * sizeof(double) + 2 * BG_MAXB;
 }
 
 cudaError_t batch_gemm_launch(const BatchGemmDesc *probs, const BatchTile *tiles, int ntiles, int *next, int ctas,

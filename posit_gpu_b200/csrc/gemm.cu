@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     double *As = reinterpret_cast<double *>(smem_raw);
     double *Ts = As + STAGES * BK * BM;
-    uint32_t *ctab = reinterpret_cast<uint32_t *>(Ts + STAGES * BK * BN); // rounding constants (F64ConstTable)
+    double *ctab = Ts + STAGES * BK * BN; // rounding constants (F64ConstTable8)
     __shared__ __align__(8) uint64_t full[STAGES];
 
     const int tid = threadIdx.x;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(NTHREADS, MIN_CTAS_PER_SM)
         mbar_fence_init();
     }
     for (int i = tid; i < F64_CONST_ENTRIES; i += NTHREADS)
-        ctab[i] = f64_round_const_top(i);
+        ctab[i] = f64_from_hi(f64_round_const_top(i));
     __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < STAGES && s < KT; ++s) {
@@ -421,7 +421,7 @@ static cudaError_t gemm_launch_impl(bool nota, bool notb, int m, int n, int k, u
     decode_a_kernel<<<grid_for(na, 256), 256, 0, stream>>>(nota, m, k, A, (size_t)lda, p.kt, na, Ad, row_nar);
     decode_b_kernel<<<grid_for(nb, 256), 256, 0, stream>>>(notb, k, n, B, (size_t)ldb, !dot, alpha, p.kt, nb,
                                                            Td, col_nar);
-    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(double) + (size_t)F64_CONST_ENTRIES * sizeof(uint32_t);
+    const size_t smem = (size_t)STAGES * BK * (BM + BN) * sizeof(double) + (size_t)F64_CONST_ENTRIES * sizeof(double);
     dim3 grid(p.mt, p.nt);
     e = dot ? cudaFuncSetAttribute(gemm_main_kernel<true, TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem)

@@ -41,7 +41,7 @@ __device__ __forceinline__ void load_operands(const double *as, const double *ts
 // nxt = cur + t*a for every accumulator; true when any step was flagged.
 template <int TM_, int TN_>
 __device__ __forceinline__ bool step_all(const double (&cur)[TM_][TN_], double (&nxt)[TM_][TN_],
-                                         const double (&a)[TM_], const double (&t)[TN_], F64ConstTable cof)
+                                         const double (&a)[TM_], const double (&t)[TN_], F64ConstTable8 cof)
 {
     bool any = false;
 #pragma unroll
@@ -59,7 +59,7 @@ __device__ __forceinline__ bool step_all(const double (&cur)[TM_][TN_], double (
 // The flagged steps of step_all(cur -> nxt), found again and redone exactly.
 template <int TM_, int TN_>
 __device__ __forceinline__ void step_fixup(const double (&cur)[TM_][TN_], double (&nxt)[TM_][TN_],
-                                           const double (&a)[TM_], const double (&t)[TN_], F64ConstTable cof)
+                                           const double (&a)[TM_], const double (&t)[TN_], F64ConstTable8 cof)
 {
 #pragma unroll
     for (int i = 0; i < TM_; ++i) {
@@ -75,9 +75,9 @@ __device__ __forceinline__ void step_fixup(const double (&cur)[TM_][TN_], double
 
 template <int TM_, int TN_>
 __device__ __forceinline__ void tile_steps_f64(double (&acc)[TM_][TN_], const double *as, const double *ts,
-                                               int lmax, const uint32_t *ctab, int tx, int ty)
+                                               int lmax, const double *ctab, int tx, int ty)
 {
-    const F64ConstTable cof{ctab};
+    const F64ConstTable8 cof{ctab};
     double alt[TM_][TN_];
     int l = 0;
     for (; l + 2 <= lmax; l += 2) {

@@ -651,10 +651,17 @@ PG_HD uint32_t f64_round_const_top(uint32_t top)
 constexpr int F64_CONST_ENTRIES = 4096;
 struct F64ConstTable {
     const uint32_t *tab;
-    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(tab[f64_hi(x) >> 20]); }
+    PG_HD_MEMBER uint32_t hi(double x) const { return tab[f64_hi(x) >> 20]; }
+    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(hi(x)); }
+};
+struct F64ConstTable8 {
+    const double *tab;
+    PG_HD_MEMBER uint32_t hi(double x) const { return f64_hi(tab[f64_hi(x) >> 20]); }
+    PG_HD_MEMBER double operator()(double x) const { return tab[f64_hi(x) >> 20]; }
 };
 struct F64ConstComputed {
-    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(f64_round_const_top(f64_hi(x) >> 20)); }
+    PG_HD_MEMBER uint32_t hi(double x) const { return f64_round_const_top(f64_hi(x) >> 20); }
+    PG_HD_MEMBER double operator()(double x) const { return f64_from_hi(hi(x)); }
 };
 
 // c + t*a with both roundings (p32_mul, kernel_entry.cl:399-538, then p32_add,
@@ -665,8 +672,9 @@ struct F64ConstComputed {
 //   s = c + q                 the FP64 sum, tested for exactness: s - c == q and s - q == c
 //                             (Fast2Sum on the larger operand makes an inexact s fail it);
 //   r = (s + Cs) - Cs         the exact sum rounded to the posit grid of its binade.
-// `fail` is set when the step must be done exactly instead: an inexact FP64 sum, or a
-// product or sum outside the fast window (its constant is NaN, so r is).
+// `fail` is set when the step must be done exactly instead: an inexact FP64 sum (a
+// product outside the fast window has a NaN constant, so q and s are NaN and fail the
+// test), or a sum outside the fast window (its table entry is the NaN marker).
 // Flagging every inexact sum is conservative: beyond 30 binades the rounded sum would be
 // right anyway, but that case is rare on the data the GEMM sees.
 template <class ConstOf>
@@ -680,9 +688,10 @@ PG_HD double f64_posit_mac(double c, double t, double a, ConstOf const_of, bool 
     // s - larger is exact (Dekker's Fast2Sum), so an inexact s leaves that difference
     // unequal to the smaller operand
     const bool inexact = (f64_add(s, -c) != q) | (f64_add(s, -q) != c);
-    const double Cs = const_of(s);
+    const uint32_t cs_hi = const_of.hi(s);
+    const double Cs = f64_from_hi(cs_hi);
     const double r = f64_add(f64_add(s, Cs), -Cs);
-    fail = inexact | (r != r);
+    fail = inexact | (cs_hi == 0x7FF80000u); // the sum's binade is outside the fast window
     return r;
 }
 
