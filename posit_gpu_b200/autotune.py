@@ -111,7 +111,7 @@ def tune_gemm_tiles(per_bucket=150, seed=7):
     return table, detail
 
 
-def tune_panel_width(sizes=(256, 512, 1024, 2048, 4096, 8192), widths=(16, 32, 64, 128, 256), seed=11):
+def tune_panel_width(sizes=(256, 512, 1024, 2048, 4096, 8192), widths=(16, 24, 32, 48, 64, 128), seed=11):
     """Time the device LU and Cholesky for each panel width at each size."""
     import torch
 

@@ -187,67 +187,82 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
 }
 
 // ---------------------------------------------------------------------------
-// LU panel in one thread-block cluster: the per-column steps of lu_pivot_kernel +
-// lu_update_kernel -- iRamax with first-max tie-break, the interchange across the panel,
-// the scaling decision, the scaled column, the rank-1 update in the FP64 step -- in the
-// same per-element order, one launch per panel.  Up to 8 CTAs of 1024 threads (8 SMs);
-// row i of the panel belongs to thread i mod (CTAs * 1024) for the whole panel, so a thread
-// reads back only what it wrote itself, except:
-//   * the pivot candidates: each CTA's best (key, row) goes to its shared memory and every
-//     CTA reads all of them through distributed shared memory after a cluster barrier,
-//     then decides the pivot itself (the same bits everywhere);
-//   * the interchange of rows k and p, done by CTA 0 and followed by a second cluster
-//     barrier before anyone reads row k (the -u_kc) or its own rows again.
-// The cluster barriers are the hardware's (barrier.cluster, release/acquire at cluster
-// scope, all CTAs of a cluster co-scheduled).  Data another SM may have written is read
-// with ld.global.cg (L2, never a stale L1 line).  A panel too tall or too wide for this
-// to beat the many-block update runs the two-launch form instead (host side).
+// LU panel in one thread-block cluster, held in shared memory: the per-column steps of
+// lu_pivot_kernel + lu_update_kernel -- iRamax with first-max tie-break, the interchange
+// across the panel, the scaling decision, the scaled column, the rank-1 update in the FP64
+// step -- in the same per-element order, one launch per panel.  Up to 8 CTAs of 1024
+// threads (8 SMs).  Row i of the panel belongs to thread i mod (CTAs * 1024) for the whole
+// panel and lives in that thread's CTA's shared memory (R rows per thread, jb patterns
+// each), loaded once and written back once.  A thread reads back only what it wrote itself,
+// except at two points per column, each behind a hardware cluster barrier
+// (barrier.cluster, release/acquire at cluster scope; the CTAs of a cluster are
+// co-scheduled, so no barrier waits for a CTA that never runs):
+//   * the pivot candidates: each CTA's best (key, row, value) goes to its shared memory;
+//     every CTA reads all of them through distributed shared memory and decides the pivot
+//     itself (the same bits everywhere);
+//   * the interchange of rows k and p, done by CTA 0 in the owners' shared memory, after
+//     which every CTA reads row k (the -u_kc) from its owner.
+// A final cluster barrier keeps every CTA's shared memory alive until no other CTA reads it.
 // ---------------------------------------------------------------------------
 constexpr int PANEL1_THREADS = 1024;
 constexpr int PANEL1_MAX_JB = 512;
 constexpr int PANEL1_MAX_CTAS = 8;
+constexpr int PANEL1_SMEM_ENTRIES = 48; // R * jb: 4 KB of shared memory per entry per CTA
 
-__device__ __forceinline__ uint32_t ldcg(const uint32_t *p) { return __ldcg(p); }
-__device__ __forceinline__ void stcg(uint32_t *p, uint32_t v) { __stcg(p, v); }
-
-// Row i of the panel is thread (i mod G)'s; its first row at or after `from`.
-__device__ __forceinline__ int first_owned(int g, int G, int from) { return from + ((g - from % G) + G) % G; }
+// Entry (row i, column c) of the panel in its owner's shared memory, through the cluster.
+__device__ __forceinline__ uint32_t *panel_entry(cooperative_groups::cluster_group &cl, uint32_t *rows, int jb,
+                                                 int G, int i, int c)
+{
+    const int g = i % G, r = i / G;
+    uint32_t *base = cl.map_shared_rank(rows, g / PANEL1_THREADS);
+    return base + ((size_t)r * jb + c) * PANEL1_THREADS + (g % PANEL1_THREADS);
+}
 
 __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
-                                                                          int M, int jb, int row0,
+                                                                          int M, int jb, int R, int row0,
                                                                           int *__restrict__ ipiv,
                                                                           int *__restrict__ info)
 {
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
+    extern __shared__ __align__(16) uint32_t s_rows[]; // [R][jb][1024]: this CTA's rows
     __shared__ int32_t s_key[32];
     __shared__ int s_idx[32];
-    __shared__ int32_t s_ckey; // this CTA's pivot candidate, read by the whole cluster:
-    __shared__ int s_cidx;     // key, row and the row's value (CTA 0's interchange may
-    __shared__ uint32_t s_cval; // overwrite the row in global memory meanwhile)
+    __shared__ uint32_t s_val[32];
+    __shared__ int32_t s_ckey; // this CTA's pivot candidate, read by the whole cluster
+    __shared__ int s_cidx;
+    __shared__ uint32_t s_cval;
     __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row, FP64
     __shared__ PivotInfo s_pi;
     if (*info < 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
+    auto own = [&](int r, int c) -> uint32_t & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
+    for (int r = 0; r < R; ++r) {
+        const int i = g + r * G;
+        if (i < M)
+            for (int c = 0; c < jb; ++c)
+                own(r, c) = P[i + (size_t)c * lda];
+    }
     for (int k = 0; k < jb; ++k) {
-        const uint32_t *col = P + (size_t)k * lda;
-        // this thread's rows of [k, M): iRamax order (iRamax.cpp:65-71), first max wins
+        // this thread's rows of [k, M) in increasing order (iRamax.cpp:65-71), first max wins
         int32_t best = INT32_MIN;
         int bidx = -1;
         uint32_t bval = 0;
-        for (int i = first_owned(g, G, k); i < M; i += G) {
-            const uint32_t v = ldcg(col + i);
-            const int32_t key = (int32_t)pabs(v);
-            if (bidx < 0 || key > best) {
-                best = key;
-                bidx = i;
-                bval = v;
+        for (int r = 0; r < R; ++r) {
+            const int i = g + r * G;
+            if (i >= k && i < M) {
+                const uint32_t v = own(r, k);
+                const int32_t key = (int32_t)pabs(v);
+                if (bidx < 0 || key > best) {
+                    best = key;
+                    bidx = i;
+                    bval = v;
+                }
             }
         }
-        __shared__ uint32_t s_val[32];
 #pragma unroll
         for (int round = 0; round < 2; ++round) {
 #pragma unroll
@@ -278,7 +293,7 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
             s_cidx = bidx;
             s_cval = bval;
         }
-        cluster.sync(); // candidates visible; every row of column k is final
+        cluster.sync(); // candidates visible
         if (tid == 0) {
             int p = -1;
             int32_t pk = INT32_MIN;
@@ -315,26 +330,34 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
         const PivotInfo pi = s_pi;
         if (rank == 0 && pi.piv != 0 && pi.row != k) { // Rgetrf2.cpp:107-117
             for (int c = tid; c < jb; c += PANEL1_THREADS) {
-                uint32_t *pc = P + (size_t)c * lda;
-                const uint32_t t = ldcg(pc + k);
-                stcg(pc + k, ldcg(pc + pi.row));
-                stcg(pc + pi.row, t);
+                uint32_t *ek = panel_entry(cluster, s_rows, jb, G, k, c);
+                uint32_t *ep = panel_entry(cluster, s_rows, jb, G, pi.row, c);
+                const uint32_t t = *ek;
+                *ek = *ep;
+                *ep = t;
             }
         }
         cluster.sync(); // the interchange is visible
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_u[c] = -p32_to_double(ldcg(P + k + (size_t)c * lda));
+            s_u[c] = -p32_to_double(*panel_entry(cluster, s_rows, jb, G, k, c));
         __syncthreads();
-        for (int i = first_owned(g, G, k + 1); i < M; i += G) {
-            uint32_t *pik = P + i + (size_t)k * lda;
-            const uint32_t l = lu_scaled(ldcg(pik), pi);
-            stcg(pik, l);
-            const double dl = p32_to_double(l);
-            for (int c = k + 1; c < jb; ++c) { // a_ic + (-u_kc)*l_i in the FP64 step
-                uint32_t *pc = P + i + (size_t)c * lda;
-                stcg(pc, p32_from_double_exact(f64_posit_mac_checked(p32_to_double(ldcg(pc)), s_u[c], dl)));
+        for (int r = 0; r < R; ++r) {
+            const int i = g + r * G;
+            if (i > k && i < M) {
+                const uint32_t l = lu_scaled(own(r, k), pi);
+                own(r, k) = l;
+                const double dl = p32_to_double(l);
+                for (int c = k + 1; c < jb; ++c) // a_ic + (-u_kc)*l_i in the FP64 step
+                    own(r, c) = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(own(r, c)), s_u[c], dl));
             }
         }
+    }
+    cluster.sync(); // no CTA leaves while another may still read its shared memory
+    for (int r = 0; r < R; ++r) {
+        const int i = g + r * G;
+        if (i < M)
+            for (int c = 0; c < jb; ++c)
+                P[i + (size_t)c * lda] = own(r, c);
     }
 }
 
@@ -796,32 +819,41 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
     }
 }
 
-// Lower Cholesky panel in one thread-block cluster, the counterpart of chol_diag_kernel +
-// chol_update_kernel, with the same row ownership and reads as lu_panel_cluster_kernel: per
-// column a cluster barrier, every CTA reads the final a_kk and takes its square root and
-// reciprocal (Rpotrf2.cpp:90-97; the same bits everywhere), each thread scales its rows
-// below the diagonal (Rtrsm.cpp:265-268), a cluster barrier, CTA 0 stores l_kk (no CTA
-// reads a_kk after that barrier), the -l_ck of the panel rows into shared memory, the
-// rank-1 update of each thread's rows.
+// Lower Cholesky panel in one thread-block cluster, held in shared memory with the same
+// row ownership as lu_panel_cluster_kernel, the counterpart of chol_diag_kernel +
+// chol_update_kernel.  Per column: a cluster barrier; every CTA reads the final a_kk from
+// its owner and takes its square root and reciprocal (Rpotrf2.cpp:90-97; the same bits
+// everywhere); each thread scales its rows below the diagonal (Rtrsm.cpp:265-268); a
+// cluster barrier; CTA 0 stores l_kk with its owner (no CTA reads a_kk after that
+// barrier); every CTA reads the panel rows' -l_ck; each thread updates its rows.  A
+// failed diagonal (info) ends the loop in every CTA at the same column; the rows are
+// written back either way.
 __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
-                                                                            int M, int jb, int row0,
+                                                                            int M, int jb, int R, int row0,
                                                                             int *__restrict__ info)
 {
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
-    __shared__ double s_l[PANEL1_MAX_JB]; // -l_ck of the current column, FP64
+    extern __shared__ __align__(16) uint32_t s_rows[]; // [R][jb][1024]: this CTA's rows
+    __shared__ double s_l[PANEL1_MAX_JB];             // -l_ck of the current column, FP64
     __shared__ uint32_t s_recip, s_lkk;
     __shared__ int s_stop;
     if (*info != 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x;
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
+    auto own = [&](int r, int c) -> uint32_t & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
+    for (int r = 0; r < R; ++r) {
+        const int i = g + r * G;
+        if (i < M)
+            for (int c = 0; c < jb; ++c)
+                own(r, c) = P[i + (size_t)c * lda];
+    }
     for (int k = 0; k < jb; ++k) {
-        uint32_t *pk = P + (size_t)k * lda;
         cluster.sync(); // every update of column k is done
         if (tid == 0) {
-            const uint32_t akk = ldcg(pk + k);
+            const uint32_t akk = *panel_entry(cluster, s_rows, jb, G, k, k);
             s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
             if (s_stop) {
                 if (rank == 0)
@@ -833,24 +865,35 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
         }
         __syncthreads();
         if (s_stop) // decided from the same a_kk in every CTA
-            return;
+            break;
         const uint32_t recip = s_recip;
-        for (int i = first_owned(g, G, k + 1); i < M; i += G)
-            stcg(pk + i, pmul(recip, ldcg(pk + i)));
+        for (int r = 0; r < R; ++r) {
+            const int i = g + r * G;
+            if (i > k && i < M)
+                own(r, k) = pmul(recip, own(r, k));
+        }
         cluster.sync(); // the scaled column is visible, and every CTA has read a_kk
         if (rank == 0 && tid == 0)
-            stcg(pk + k, s_lkk);
+            *panel_entry(cluster, s_rows, jb, G, k, k) = s_lkk;
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_l[c] = -p32_to_double(ldcg(pk + c));
+            s_l[c] = -p32_to_double(*panel_entry(cluster, s_rows, jb, G, c, k));
         __syncthreads();
-        for (int i = first_owned(g, G, k + 1); i < M; i += G) {
-            const double dl = p32_to_double(ldcg(pk + i));
-            const int cend = min(jb - 1, i);
-            for (int c = k + 1; c <= cend; ++c) { // a_ic + (-l_ck)*l_i in the FP64 step
-                uint32_t *pc = P + i + (size_t)c * lda;
-                stcg(pc, p32_from_double_exact(f64_posit_mac_checked(p32_to_double(ldcg(pc)), s_l[c], dl)));
+        for (int r = 0; r < R; ++r) {
+            const int i = g + r * G;
+            if (i > k && i < M) {
+                const double dl = p32_to_double(own(r, k));
+                const int cend = min(jb - 1, i);
+                for (int c = k + 1; c <= cend; ++c) // a_ic + (-l_ck)*l_i in the FP64 step
+                    own(r, c) = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(own(r, c)), s_l[c], dl));
             }
         }
+    }
+    cluster.sync(); // l_kk stored; no CTA leaves while another may still read its shared memory
+    for (int r = 0; r < R; ++r) {
+        const int i = g + r * G;
+        if (i < M)
+            for (int c = 0; c < jb; ++c)
+                P[i + (size_t)c * lda] = own(r, c);
     }
 }
 
@@ -995,29 +1038,39 @@ size_t rgetrf_workspace_bytes(int m, int n, int nb)
     return panel_ws_bytes(m) + g;
 }
 
-// The panel form: CTAs of a cluster panel (1..8, one per 1024 rows), or 0 for the
-// two-launch form.  A cluster panel's column costs two cluster barriers plus the rank-1
-// update of its rows on at most 8 SMs; the two-launch form costs two dependent launches
-// (about 7 microseconds each) with the update spread over all SMs.  The crossover, about
-// 1.5e-5 microseconds per panel entry against 12 microseconds, is at M*jb ~ 8e5.
-static int panel_cluster_ctas(int M, int jb)
+// The panel form: the cluster panel held in shared memory when its rows fit (ncta CTAs,
+// one per 1024 rows up to 8, R rows per thread, R * jb <= PANEL1_SMEM_ENTRIES), else the
+// two-launch form (ncta = 0).
+struct PanelForm {
+    int ncta, R;
+};
+static PanelForm panel_form(int M, int jb)
 {
-    if (jb > PANEL1_MAX_JB || (long long)M * jb > 800000LL)
-        return 0;
-    return std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_THREADS - 1) / PANEL1_THREADS));
+    if (jb > PANEL1_MAX_JB)
+        return {0, 0};
+    const int ncta = std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_THREADS - 1) / PANEL1_THREADS));
+    const int G = ncta * PANEL1_THREADS, R = (M + G - 1) / G;
+    if (R * jb > PANEL1_SMEM_ENTRIES)
+        return {0, 0};
+    return {ncta, R};
 }
 
 template <class... Args>
-static cudaError_t launch_panel_cluster(void (*kernel)(Args...), int ncta, cudaStream_t st, Args... args)
+static cudaError_t launch_panel_cluster(void (*kernel)(Args...), PanelForm f, int jb, cudaStream_t st, Args... args)
 {
+    const size_t smem = (size_t)f.R * jb * PANEL1_THREADS * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         PANEL1_SMEM_ENTRIES * PANEL1_THREADS * (int)sizeof(uint32_t));
+    if (e != cudaSuccess)
+        return e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)ncta);
+    cfg.gridDim = dim3((unsigned)f.ncta);
     cfg.blockDim = dim3(PANEL1_THREADS);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)ncta;
+    attr[0].val.clusterDim.x = (unsigned)f.ncta;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
@@ -1048,9 +1101,9 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         const int M = m - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j; // indexed by panel-local row
-        const int ncta = panel_cluster_ctas(M, jb);
-        if (ncta > 0) {
-            cudaError_t e = launch_panel_cluster(lu_panel_cluster_kernel, ncta, st, P, L, M, jb, j, ipiv, info);
+        const PanelForm pf = panel_form(M, jb);
+        if (pf.ncta > 0) {
+            cudaError_t e = launch_panel_cluster(lu_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, ipiv, info);
             if (e != cudaSuccess)
                 return e;
         } else {
@@ -1104,9 +1157,9 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         const int M = n - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j;
-        const int ncta = panel_cluster_ctas(M, jb);
-        if (ncta > 0) {
-            cudaError_t e = launch_panel_cluster(chol_panel_cluster_kernel, ncta, st, P, L, M, jb, j, info);
+        const PanelForm pf = panel_form(M, jb);
+        if (pf.ncta > 0) {
+            cudaError_t e = launch_panel_cluster(chol_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, info);
             if (e != cudaSuccess)
                 return e;
         } else {
