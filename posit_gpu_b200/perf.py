@@ -19,16 +19,16 @@ SM_MAX_MHZ = 1965.0
 
 # Warp instructions issued by gemm_main_kernel per posit multiply-add:
 # smsp__inst_executed.sum / (m*n*k) for one NN launch at m = n = k = 4096
-# (50,306,712,730 / 68,719,476,736 = 0.7321, i.e. 23.43 thread instructions).  Of those,
-# 11 per multiply-add run on the FP64 pipe (DMUL, DFMA, 7 DADD, 2 DSETP): FP64 pipe
-# 66.0 %, ALU pipe 28.5 %, LSU 29.4 %, issue 70.7 % busy in the same capture.
-WARP_INST_PER_MAD = 0.7321
-FP64_WARP_INST_PER_MAD = 11 / 32
+# (48,162,455,398 / 68,719,476,736 = 0.7009, i.e. 22.43 thread instructions).  Of those,
+# 10 per multiply-add run on the FP64 pipe (DMUL, DFMA, 6 DADD, 2 DSETP): FP64 pipe
+# 62.9 %, ALU pipe 36.1 %, LSU 30.8 %, issue 70.9 % busy in the same capture.
+WARP_INST_PER_MAD = 0.7009
+FP64_WARP_INST_PER_MAD = 10 / 32
 INST_SOURCE = ("ncu --set full, gemm_main_kernel<0,0>, NN 4096^3 U[-1,1] "
                "(profiles/gemm_main_kernel_nn_4096.md)")
 # DRAM bytes (read + write) per posit multiply-add of the same launch:
-# (7,468,817,000 + 72,625,152) / 68,719,476,736.
-MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1097
+# (7,488,873,000 + 121,976,832) / 68,719,476,736.
+MAIN_KERNEL_DRAM_BYTES_PER_MAD = 0.1108
 
 
 def issue_peak_warp_inst_per_s(sm_mhz):
@@ -45,7 +45,7 @@ def fp64_pipe_peak_warp_inst_per_s(sm_mhz):
 # the script that compiles them (flags included); the benchmark recomputes the digest and,
 # when it differs, marks the count stale and reports no roofline fraction from it.
 KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh", "build.py"]
-INST_SOURCE_DIGEST = "dc10a8365209bb53992d6ac760cc868b8276bb1b8d3380037f399a616ddbd161"
+INST_SOURCE_DIGEST = "fd6a4f522a9b6bbf01d2d31ebff5027198484163ca5c409e99bdad6ddd871c27"
 
 
 def kernel_source_digest():

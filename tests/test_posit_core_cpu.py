@@ -355,7 +355,7 @@ def test_scan_form_of_the_chain_matches_sequential_additions(hc):
         else:  # addends 24..31 binades below a running value near 1
             q = oracle.from_double(rng.choice([-1, 1], n) * 2.0 ** -rng.integers(24, 32, n) * rng.uniform(1, 2, n))
         c0 = int(oracle.from_double(np.array([rng.uniform(-2, 2)]))[0])
-        E = int(rng.choice([1, 2, 4, 8]))
+        E = int(rng.choice([1, 2, 4, 8, 16]))  # 16: a 512-term window, as four warps of 32 lanes x 4 scan
         assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
         assert hc.hc_chain_reg_check(c0, np.ascontiguousarray(q), n) == 1, (trial, kind, n, "reg")
     assert stats[0] > 0 and stats[1] > 0  # both scans and exact steps were exercised
