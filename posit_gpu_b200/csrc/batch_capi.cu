@@ -124,7 +124,7 @@ static int size_bucket(int x) { return x <= 32 ? 0 : (x <= 64 ? 1 : 2); }
 // Default tile-shape table (rows: m bucket <=32, <=64, >64; columns: n bucket), used
 // when the caller passes none: 32x32 for small problems, 32x64 for short-and-wide ones,
 // 64x32 otherwise.
-static const int kDefaultTileTable[9] = {1, 2, 2, 0, 0, 0, 0, 0, 0};
+static const int kDefaultTileTable[9] = {1, 1, 1, 1, 1, 0, 1, 1, 2}; // tuning_b200.json
 
 extern "C" int posit_batch_gemm_plan_create(const posit_batch_gemm *probs, int nprob, const int *tile_table,
                                             posit_batch_plan **out, int *bad_index)

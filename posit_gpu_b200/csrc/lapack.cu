@@ -736,6 +736,196 @@ __global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint3
         bcol[k] = s_b[k];
 }
 
+// ---------------------------------------------------------------------------
+// The same solve with the row's windows spread over a group of warps.
+// ---------------------------------------------------------------------------
+// One block of 2 * LLT_GROUP_WARPS warps per right-hand side: the first LLT_GROUP_WARPS
+// warps (the consumer group) sum each row in windows of LLT_GROUP_WARPS * 32 * LLT_SCAN_E
+// terms; the others compute the next row's terms meanwhile, as in trsm_llt_pc_kernel.  A
+// window is the warp scan of step maps in every consumer warp, then each warp's composed map
+// goes to shared memory, a named barrier (the consumer group only), each warp composes the
+// maps of the warps before it with its own exclusive prefix and walks its addends, each warp
+// reports its first step the scan form does not cover, a named barrier, and every consumer
+// thread takes the first such step of the window (or the window's end value).  Every
+// consumer thread then holds the same running value; the exact steps and the sequential
+// runs after a window cut short run in every consumer thread alike (no broadcast needed).
+constexpr int LLT_GROUP_WARPS = 4;
+constexpr int LLT_GROUP_THREADS = 2 * LLT_GROUP_WARPS * 32;
+
+struct GroupScan {
+    SegFn wt[LLT_GROUP_WARPS]; // each consumer warp's composed map
+    int jbad[LLT_GROUP_WARPS]; // each warp's first uncovered step (-1: none)
+    int32_t Mbad[LLT_GROUP_WARPS];
+    int32_t Mend; // M after the window's last addend
+};
+
+__device__ __forceinline__ void group_bar() { asm volatile("bar.sync 1, %0;" ::"r"(LLT_GROUP_WARPS * 32) : "memory"); }
+
+template <int E, class Q>
+__device__ double group_chain_scan(double t, Q q, int pos, int end, GroupScan *gs)
+{
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    const int ct = threadIdx.x, lane = ct & 31, w = ct >> 5;
+    while (pos < end) {
+        SegParams sp;
+        if (!seg_begin(t, sp)) { // zero, or outside the fast window: one exact step
+            t = chain_add_one(t, q[pos]);
+            ++pos;
+            continue;
+        }
+        const int wend = min(end, pos + LLT_GROUP_WARPS * 32 * E);
+        const int j0 = pos + ct * E;
+        SegFn fe[E];
+        int32_t K[E];
+        bool rk[E];
+        SegFn f = {0, 0};
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double qv = j0 + e < wend ? q[j0 + e] : 0.0; // 0 is the identity map
+            fe[e] = seg_fn(qv, sp, K[e], rk[e]);
+            f = seg_then(f, fe[e]);
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            SegFn o;
+            o.c0 = __shfl_up_sync(FULL, f.c0, off);
+            o.c1 = __shfl_up_sync(FULL, f.c1, off);
+            if (lane >= off)
+                f = seg_then(o, f);
+        }
+        SegFn ex;
+        ex.c0 = __shfl_up_sync(FULL, f.c0, 1);
+        ex.c1 = __shfl_up_sync(FULL, f.c1, 1);
+        if (lane == 0)
+            ex = SegFn{0, 0};
+        if (lane == 31)
+            gs->wt[w] = f;
+        group_bar();
+        SegFn pre = {0, 0};
+        for (int v = 0; v < w; ++v)
+            pre = seg_then(pre, gs->wt[v]);
+        int32_t M = seg_apply(seg_then(pre, ex), sp.M0);
+        int jbad = -1;
+        int32_t Mbad = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const bool live = (jbad < 0) & (j0 + e < wend);
+            const bool ok = seg_valid(M, K[e], rk[e], sp);
+            if (live & !ok) {
+                jbad = j0 + e;
+                Mbad = M;
+            }
+            if (live & ok)
+                M = seg_apply(fe[e], M);
+        }
+        const unsigned bal = __ballot_sync(FULL, jbad >= 0);
+        if (bal == 0) {
+            if (lane == 0)
+                gs->jbad[w] = -1;
+        } else if (lane == __ffs(bal) - 1) {
+            gs->jbad[w] = jbad;
+            gs->Mbad[w] = Mbad;
+        }
+        if (ct == (wend - 1 - pos) / E) // the thread holding the window's last addend
+            gs->Mend = M;
+        group_bar();
+        int js = -1;
+        int32_t Ms = 0;
+        for (int v = 0; v < LLT_GROUP_WARPS; ++v)
+            if (gs->jbad[v] >= 0) {
+                js = gs->jbad[v];
+                Ms = gs->Mbad[v];
+                break;
+            }
+        const int32_t Me = gs->Mend;
+        group_bar(); // every consumer has read the window's results before the next one
+        if (js < 0) {
+            t = sp.us * (double)Me;
+            pos = wend;
+        } else {
+            t = chain_add_one(sp.us * (double)Ms, q[js]);
+            const bool cut_short = js - pos < LLT_SHORT_WINDOW;
+            pos = js + 1;
+            if (cut_short) {
+                const int cnt = min(LLT_SEQ_STEPS, end - pos);
+                t = chain_add_run_reg(t, q + pos, cnt);
+                pos += cnt;
+            }
+        }
+    }
+    return t;
+}
+
+template <class T, bool UPPER = false>
+__global__ void __launch_bounds__(LLT_GROUP_THREADS) trsm_ltx_group_kernel(const uint32_t *__restrict__ L,
+                                                                           size_t ldl, uint32_t *__restrict__ B,
+                                                                           size_t ldb, int m, bool unit,
+                                                                           const int *__restrict__ info)
+{
+    extern __shared__ __align__(16) unsigned char smem_pc[];
+    T *s_q = reinterpret_cast<T *>(smem_pc); // [2][m]: terms
+    uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
+    __shared__ uint32_t s_nar[2];
+    __shared__ GroupScan s_gs;
+    if (info && *info != 0) // a factorization stopped before this solve
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    const int tid = threadIdx.x;
+    constexpr int NC = LLT_GROUP_WARPS * 32; // consumer threads
+    for (int k = tid; k < m; k += LLT_GROUP_THREADS)
+        s_b[k] = bcol[k];
+    if (tid < 2)
+        s_nar[tid] = 0;
+    __syncthreads();
+    uint32_t xprev = 0; // the row finished last, b_{i+1} (lower) or b_{i-1} (upper) (consumers)
+    for (int step = 0; step < m; ++step) {
+        const int i = UPPER ? step : m - 1 - step;
+        const int cur = step & 1;
+        if (tid < NC) {
+            const uint32_t *li = L + (size_t)i * ldl;
+            const uint32_t bi = s_b[i];
+            uint32_t nar = (bi == P32_NAR) | s_nar[cur];
+            double c = p32_to_double(bi == P32_NAR ? 0u : bi);
+            const typename LltTerms<T>::View q{s_q + (size_t)cur * m};
+            if (!UPPER && i + 1 < m) {
+                c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
+                c = group_chain_scan<LLT_SCAN_E>(c, q, i + 2, m, &s_gs);
+            }
+            if (UPPER && i >= 1) {
+                c = group_chain_scan<LLT_SCAN_E>(c, q, 0, i - 1, &s_gs);
+                c = chain_add_one(c, llt_term(li[i - 1], xprev, &nar));
+            }
+            uint32_t t = nar ? P32_NAR : p32_from_double(c);
+            if (!unit)
+                t = pdiv(t, li[i]);
+            xprev = t;
+            group_bar(); // every consumer has read s_nar[cur]
+            if (tid == 0) {
+                s_b[i] = t;
+                s_nar[cur] = 0;
+            }
+        } else if (step + 1 < m) {
+            // the terms of the next row whose b_k are final: k = i+1 .. m-1 of row i-1
+            // (lower), k = 0 .. i-1 of row i+1 (upper)
+            const int nxt = UPPER ? i + 1 : i - 1;
+            const int kbeg = UPPER ? 0 : i + 1, kend = UPPER ? i : m;
+            const uint32_t *lp = L + (size_t)nxt * ldl;
+            T *qn = s_q + (size_t)(cur ^ 1) * m;
+            uint32_t nar = 0;
+            for (int k = kbeg + (tid - NC); k < kend; k += LLT_GROUP_THREADS - NC) {
+                const uint32_t p = pmul(0u - s_b[k], lp[k]); // (-b)*a == -(a*b) bit for bit
+                nar |= p == P32_NAR;
+                qn[k] = LltTerms<T>::store(p == P32_NAR ? 0u : p);
+            }
+            if (nar)
+                s_nar[cur ^ 1] = 1;
+        }
+        __syncthreads();
+    }
+    for (int k = tid; k < m; k += LLT_GROUP_THREADS)
+        bcol[k] = s_b[k];
+}
+
 size_t llt_pc_smem_bytes(int m, size_t term_bytes) { return (size_t)m * (2 * term_bytes + 4); }
 
 // ---------------------------------------------------------------------------
@@ -1020,7 +1210,7 @@ int tuned_panel_width(bool lu, int n)
         int n, lu, chol;
     };
     static const Row rows[] = {{0, 16, 16}, {512, 16, 16}, {1024, 16, 16}, {2048, 16, 16}, {4096, 16, 16},
-                               {8192, 16, 16}};
+                               {8192, 128, 16}};
     int nb = 16;
     for (const Row &r : rows)
         if (n >= r.n)
@@ -1294,23 +1484,23 @@ static cudaError_t launch_ltx(bool upper, bool unit, int n, int nrhs, const uint
     if (pc8 <= (size_t)LLT_SMEM_MAX || pc4 <= (size_t)LLT_SMEM_MAX) {
         const bool f64 = pc8 <= (size_t)LLT_SMEM_MAX;
         const size_t pc = f64 ? pc8 : pc4;
-        const void *fn = f64 ? (upper ? (const void *)trsm_llt_pc_kernel<double, true>
-                                      : (const void *)trsm_llt_pc_kernel<double, false>)
-                             : (upper ? (const void *)trsm_llt_pc_kernel<uint32_t, true>
-                                      : (const void *)trsm_llt_pc_kernel<uint32_t, false>);
+        const void *fn = f64 ? (upper ? (const void *)trsm_ltx_group_kernel<double, true>
+                                      : (const void *)trsm_ltx_group_kernel<double, false>)
+                             : (upper ? (const void *)trsm_ltx_group_kernel<uint32_t, true>
+                                      : (const void *)trsm_ltx_group_kernel<uint32_t, false>);
         if (pc > 48 * 1024) {
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc);
             if (e != cudaSuccess)
                 return e;
         }
         if (f64 && upper)
-            trsm_llt_pc_kernel<double, true><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+            trsm_ltx_group_kernel<double, true><<<nrhs, LLT_GROUP_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         else if (f64)
-            trsm_llt_pc_kernel<double, false><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+            trsm_ltx_group_kernel<double, false><<<nrhs, LLT_GROUP_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         else if (upper)
-            trsm_llt_pc_kernel<uint32_t, true><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+            trsm_ltx_group_kernel<uint32_t, true><<<nrhs, LLT_GROUP_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         else
-            trsm_llt_pc_kernel<uint32_t, false><<<nrhs, LLT_PC_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
+            trsm_ltx_group_kernel<uint32_t, false><<<nrhs, LLT_GROUP_THREADS, pc, st>>>(A, lda, B, ldb, n, unit, info);
         return cudaGetLastError();
     }
     const size_t col = (size_t)n * 4;
