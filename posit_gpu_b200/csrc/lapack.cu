@@ -207,16 +207,29 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
 constexpr int PANEL1_THREADS = 1024;
 constexpr int PANEL1_MAX_JB = 512;
 constexpr int PANEL1_MAX_CTAS = 8;
-constexpr int PANEL1_SMEM_ENTRIES = 48; // R * jb: 4 KB of shared memory per entry per CTA
+constexpr int PANEL1_SMEM_ENTRIES = 24; // R * jb: 8 KB of shared memory (1024 FP64 values) per entry per CTA
 
 // Entry (row i, column c) of the panel in its owner's shared memory, through the cluster.
-__device__ __forceinline__ uint32_t *panel_entry(cooperative_groups::cluster_group &cl, uint32_t *rows, int jb,
-                                                 int G, int i, int c)
+__device__ __forceinline__ double *panel_entry(cooperative_groups::cluster_group &cl, double *rows, int jb, int G,
+                                               int i, int c)
 {
     const int g = i % G, r = i / G;
-    uint32_t *base = cl.map_shared_rank(rows, g / PANEL1_THREADS);
+    double *base = cl.map_shared_rank(rows, g / PANEL1_THREADS);
     return base + ((size_t)r * jb + c) * PANEL1_THREADS + (g % PANEL1_THREADS);
 }
+
+// The barrier of a cluster panel: the cluster's, or the block's when the cluster is one CTA.
+__device__ __forceinline__ void panel_sync(cooperative_groups::cluster_group &cl, int ncta)
+{
+    if (ncta == 1)
+        __syncthreads();
+    else
+        cl.sync();
+}
+
+// Pivot key of an FP64-held posit value: |x|, NaR (NaN) below everything, the order of
+// pabs() on patterns (iRamax.cpp:65-71 compares abs() in posit order).
+__device__ __forceinline__ double pivot_key(double x) { return x != x ? -1.0 : fabs(x); }
 
 __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
                                                                           int M, int jb, int R, int row0,
@@ -226,36 +239,32 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
-    extern __shared__ __align__(16) uint32_t s_rows[]; // [R][jb][1024]: this CTA's rows
-    __shared__ int32_t s_key[32];
+    extern __shared__ __align__(16) double s_rows[]; // [R][jb][1024]: this CTA's rows, FP64
+    __shared__ double s_key[32], s_val[32];
     __shared__ int s_idx[32];
-    __shared__ uint32_t s_val[32];
-    __shared__ int32_t s_ckey; // this CTA's pivot candidate, read by the whole cluster
-    __shared__ int s_cidx;
-    __shared__ uint32_t s_cval;
-    __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row, FP64
+    __shared__ double s_ckey, s_cval; // this CTA's pivot candidate (key, value, row), read by
+    __shared__ int s_cidx;            // the whole cluster
+    __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row
     __shared__ PivotInfo s_pi;
     if (*info < 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
-    auto own = [&](int r, int c) -> uint32_t & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
+    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
     for (int r = 0; r < R; ++r) {
         const int i = g + r * G;
         if (i < M)
             for (int c = 0; c < jb; ++c)
-                own(r, c) = P[i + (size_t)c * lda];
+                own(r, c) = p32_to_double(P[i + (size_t)c * lda]);
     }
     for (int k = 0; k < jb; ++k) {
         // this thread's rows of [k, M) in increasing order (iRamax.cpp:65-71), first max wins
-        int32_t best = INT32_MIN;
+        double best = -2.0, bval = 0.0;
         int bidx = -1;
-        uint32_t bval = 0;
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i >= k && i < M) {
-                const uint32_t v = own(r, k);
-                const int32_t key = (int32_t)pabs(v);
+                const double v = own(r, k), key = pivot_key(v);
                 if (bidx < 0 || key > best) {
                     best = key;
                     bidx = i;
@@ -267,9 +276,9 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
         for (int round = 0; round < 2; ++round) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
-                const int32_t k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
+                const double k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
+                const double v2 = __shfl_down_sync(0xFFFFFFFFu, bval, off);
                 const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
-                const uint32_t v2 = __shfl_down_sync(0xFFFFFFFFu, bval, off);
                 if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
                     best = k2;
                     bidx = i2;
@@ -293,20 +302,20 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
             s_cidx = bidx;
             s_cval = bval;
         }
-        cluster.sync(); // candidates visible
+        panel_sync(cluster, ncta); // candidates visible
         if (tid == 0) {
             int p = -1;
-            int32_t pk = INT32_MIN;
-            uint32_t piv = 0;
+            double pk = -2.0, pv = 0.0;
             for (int r = 0; r < ncta; ++r) {
-                const int32_t k2 = *cluster.map_shared_rank(&s_ckey, r);
+                const double k2 = *cluster.map_shared_rank(&s_ckey, r);
                 const int i2 = *cluster.map_shared_rank(&s_cidx, r);
                 if (i2 >= 0 && (p < 0 || k2 > pk || (k2 == pk && i2 < p))) {
                     pk = k2;
                     p = i2;
-                    piv = *cluster.map_shared_rank(&s_cval, r);
+                    pv = *cluster.map_shared_rank(&s_cval, r); // the row itself may move meanwhile
                 }
             }
+            const uint32_t piv = p32_from_double_exact(pv);
             PivotInfo pi;
             pi.row = p;
             pi.piv = piv;
@@ -330,35 +339,113 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
         const PivotInfo pi = s_pi;
         if (rank == 0 && pi.piv != 0 && pi.row != k) { // Rgetrf2.cpp:107-117
             for (int c = tid; c < jb; c += PANEL1_THREADS) {
-                uint32_t *ek = panel_entry(cluster, s_rows, jb, G, k, c);
-                uint32_t *ep = panel_entry(cluster, s_rows, jb, G, pi.row, c);
-                const uint32_t t = *ek;
+                double *ek = panel_entry(cluster, s_rows, jb, G, k, c);
+                double *ep = panel_entry(cluster, s_rows, jb, G, pi.row, c);
+                const double t = *ek;
                 *ek = *ep;
                 *ep = t;
             }
         }
-        cluster.sync(); // the interchange is visible
+        panel_sync(cluster, ncta); // the interchange is visible
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_u[c] = -p32_to_double(*panel_entry(cluster, s_rows, jb, G, k, c));
+            s_u[c] = -*panel_entry(cluster, s_rows, jb, G, k, c);
         __syncthreads();
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i > k && i < M) {
-                const uint32_t l = lu_scaled(own(r, k), pi);
-                own(r, k) = l;
+                const uint32_t l = lu_scaled(p32_from_double_exact(own(r, k)), pi);
                 const double dl = p32_to_double(l);
+                own(r, k) = dl;
                 for (int c = k + 1; c < jb; ++c) // a_ic + (-u_kc)*l_i in the FP64 step
-                    own(r, c) = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(own(r, c)), s_u[c], dl));
+                    own(r, c) = f64_posit_mac_checked(own(r, c), s_u[c], dl);
             }
         }
     }
-    cluster.sync(); // no CTA leaves while another may still read its shared memory
+    panel_sync(cluster, ncta); // no CTA leaves while another may still read its shared memory
     for (int r = 0; r < R; ++r) {
         const int i = g + r * G;
         if (i < M)
             for (int c = 0; c < jb; ++c)
-                P[i + (size_t)c * lda] = own(r, c);
+                P[i + (size_t)c * lda] = p32_from_double_exact(own(r, c));
     }
+}
+
+// After a panel of columns [j, j+jb) (jb <= ROWS_JB_MAX): the panel's row interchanges
+// (Rlaswp, Rlaswp.cpp:77-107, in ascending order) on every column outside the panel, and
+// the unit-lower solve of the U12 block (Rtrsm('L', 'L', 'N', 'U'), Rtrsm.cpp:139-154, zero
+// multipliers skipped as there) on the columns right of it, in one launch: one thread per
+// column, its rows j..j+jb-1 and the interchanges' other rows held in registers (loaded
+// together, so one memory latency per column instead of one per interchange).
+constexpr int ROWS_JB_MAX = 32;
+constexpr int ROWS_THREADS = 128;
+
+__global__ void __launch_bounds__(ROWS_THREADS) lu_rows_kernel(uint32_t *__restrict__ A, size_t lda, int n, int j,
+                                                               int jb, const int *__restrict__ ipiv)
+{
+    __shared__ double s_L[ROWS_JB_MAX * ROWS_JB_MAX]; // l_ik at [i * ROWS_JB_MAX + k], FP64
+    __shared__ int s_t[ROWS_JB_MAX];                  // interchange i: row j+i <-> row s_t[i] (0-based)
+    __shared__ int s_alias[ROWS_JB_MAX];              // below the block: the first interchange with that row
+    const int tid = threadIdx.x;
+    for (int e = tid; e < jb * jb; e += ROWS_THREADS) {
+        const int i = e % jb, k = e / jb;
+        s_L[i * ROWS_JB_MAX + k] = p32_to_double(A[(j + i) + (size_t)(j + k) * lda]);
+    }
+    for (int i = tid; i < jb; i += ROWS_THREADS)
+        s_t[i] = ipiv[j + i] - 1;
+    __syncthreads();
+    for (int i = tid; i < jb; i += ROWS_THREADS) {
+        int a = -1;
+        if (s_t[i] >= j + jb) {
+            a = i;
+            for (int q = 0; q < i; ++q)
+                if (s_t[q] == s_t[i]) {
+                    a = q;
+                    break;
+                }
+        }
+        s_alias[i] = a;
+    }
+    __syncthreads();
+    const int ci = blockIdx.x * ROWS_THREADS + tid;
+    if (ci >= n - jb)
+        return;
+    const int c = ci < j ? ci : ci + jb; // the columns outside the panel
+    uint32_t *col = A + (size_t)c * lda;
+    uint32_t v[ROWS_JB_MAX], w[ROWS_JB_MAX];
+    for (int i = 0; i < jb; ++i)
+        v[i] = col[j + i];
+    for (int i = 0; i < jb; ++i)
+        if (s_alias[i] == i)
+            w[i] = col[s_t[i]];
+    for (int i = 0; i < jb; ++i) {
+        const int t = s_t[i];
+        if (t == j + i)
+            continue;
+        uint32_t *o = t < j + jb ? &v[t - j] : &w[s_alias[i]];
+        const uint32_t x = v[i];
+        v[i] = *o;
+        *o = x;
+    }
+    for (int i = 0; i < jb; ++i)
+        if (s_alias[i] == i)
+            col[s_t[i]] = w[i];
+    if (c > j) { // U12 <- L11^-1 A12, column-oriented as Rtrsm.cpp:139-154 (unit diagonal)
+        double x[ROWS_JB_MAX];
+        for (int i = 0; i < jb; ++i)
+            x[i] = p32_to_double(v[i]);
+        for (int k = 0; k < jb; ++k) {
+            const double bk = x[k];
+            if (bk != 0.0) {
+                const double nbk = -bk;
+                for (int i = k + 1; i < jb; ++i)
+                    x[i] = f64_posit_mac_checked(x[i], nbk, s_L[i * ROWS_JB_MAX + k]);
+            }
+        }
+        for (int i = 0; i < jb; ++i)
+            v[i] = p32_from_double(x[i]);
+    }
+    for (int i = 0; i < jb; ++i)
+        col[j + i] = v[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -1025,25 +1112,25 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
-    extern __shared__ __align__(16) uint32_t s_rows[]; // [R][jb][1024]: this CTA's rows
-    __shared__ double s_l[PANEL1_MAX_JB];             // -l_ck of the current column, FP64
+    extern __shared__ __align__(16) double s_rows[]; // [R][jb][1024]: this CTA's rows, FP64
+    __shared__ double s_l[PANEL1_MAX_JB];           // -l_ck of the current column
     __shared__ uint32_t s_recip, s_lkk;
     __shared__ int s_stop;
     if (*info != 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x;
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
-    auto own = [&](int r, int c) -> uint32_t & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
+    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
     for (int r = 0; r < R; ++r) {
         const int i = g + r * G;
         if (i < M)
             for (int c = 0; c < jb; ++c)
-                own(r, c) = P[i + (size_t)c * lda];
+                own(r, c) = p32_to_double(P[i + (size_t)c * lda]);
     }
     for (int k = 0; k < jb; ++k) {
-        cluster.sync(); // every update of column k is done
+        panel_sync(cluster, ncta); // every update of column k is done
         if (tid == 0) {
-            const uint32_t akk = *panel_entry(cluster, s_rows, jb, G, k, k);
+            const uint32_t akk = p32_from_double_exact(*panel_entry(cluster, s_rows, jb, G, k, k));
             s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
             if (s_stop) {
                 if (rank == 0)
@@ -1060,30 +1147,30 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i > k && i < M)
-                own(r, k) = pmul(recip, own(r, k));
+                own(r, k) = p32_to_double(pmul(recip, p32_from_double_exact(own(r, k))));
         }
-        cluster.sync(); // the scaled column is visible, and every CTA has read a_kk
+        panel_sync(cluster, ncta); // the scaled column is visible, and every CTA has read a_kk
         if (rank == 0 && tid == 0)
-            *panel_entry(cluster, s_rows, jb, G, k, k) = s_lkk;
+            *panel_entry(cluster, s_rows, jb, G, k, k) = p32_to_double(s_lkk);
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_l[c] = -p32_to_double(*panel_entry(cluster, s_rows, jb, G, c, k));
+            s_l[c] = -*panel_entry(cluster, s_rows, jb, G, c, k);
         __syncthreads();
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i > k && i < M) {
-                const double dl = p32_to_double(own(r, k));
+                const double dl = own(r, k);
                 const int cend = min(jb - 1, i);
                 for (int c = k + 1; c <= cend; ++c) // a_ic + (-l_ck)*l_i in the FP64 step
-                    own(r, c) = p32_from_double_exact(f64_posit_mac_checked(p32_to_double(own(r, c)), s_l[c], dl));
+                    own(r, c) = f64_posit_mac_checked(own(r, c), s_l[c], dl);
             }
         }
     }
-    cluster.sync(); // l_kk stored; no CTA leaves while another may still read its shared memory
+    panel_sync(cluster, ncta); // l_kk stored; no CTA leaves while another may still read its shared memory
     for (int r = 0; r < R; ++r) {
         const int i = g + r * G;
         if (i < M)
             for (int c = 0; c < jb; ++c)
-                P[i + (size_t)c * lda] = own(r, c);
+                P[i + (size_t)c * lda] = p32_from_double_exact(own(r, c));
     }
 }
 
@@ -1248,9 +1335,9 @@ static PanelForm panel_form(int M, int jb)
 template <class... Args>
 static cudaError_t launch_panel_cluster(void (*kernel)(Args...), PanelForm f, int jb, cudaStream_t st, Args... args)
 {
-    const size_t smem = (size_t)f.R * jb * PANEL1_THREADS * sizeof(uint32_t);
+    const size_t smem = (size_t)f.R * jb * PANEL1_THREADS * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         PANEL1_SMEM_ENTRIES * PANEL1_THREADS * (int)sizeof(uint32_t));
+                                         PANEL1_SMEM_ENTRIES * PANEL1_THREADS * (int)sizeof(double));
     if (e != cudaSuccess)
         return e;
     cudaLaunchConfig_t cfg = {};
@@ -1303,16 +1390,26 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
                 lu_pivot_kernel<<<1, 1024, 0, st>>>(P, L, M, jb, k + 1, j, ipiv, info, pinfo, lc, k);
             }
         }
-        if (j > 0)
-            laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
+        if (jb <= ROWS_JB_MAX) {
+            if (n > jb)
+                lu_rows_kernel<<<(n - jb + ROWS_THREADS - 1) / ROWS_THREADS, ROWS_THREADS, 0, st>>>(A, L, n, j, jb,
+                                                                                                 ipiv);
+        } else {
+            if (j > 0)
+                laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
+            if (j + jb < n) {
+                const int nr = n - j - jb;
+                laswp_kernel<<<(nr + 127) / 128, 128, 0, st>>>(A + (size_t)(j + jb) * L, L, nr, j + 1, j + jb, ipiv,
+                                                              1, info);
+                cudaError_t e = launch_lln(nr, 256, P, L, A + j + (size_t)(j + jb) * L, L, jb, true, info, st);
+                if (e != cudaSuccess)
+                    return e;
+            }
+        }
         if (j + jb < n) {
             const int nr = n - j - jb;
             uint32_t *A12 = A + j + (size_t)(j + jb) * L;
-            laswp_kernel<<<(nr + 127) / 128, 128, 0, st>>>(A + (size_t)(j + jb) * L, L, nr, j + 1, j + jb, ipiv, 1,
-                                                          info);
-            cudaError_t e = launch_lln(nr, 256, P, L, A12, L, jb, true, info, st);
-            if (e != cudaSuccess)
-                return e;
+            cudaError_t e = cudaSuccess;
             if (j + jb < m) {
                 e = gemm_launch(true, true, m - j - jb, nr, jb, 0xC0000000u /* -1 */,
                                             A + (j + jb) + (size_t)j * L, lda, A12, lda, P32_ONE,
