@@ -1297,7 +1297,7 @@ int tuned_panel_width(bool lu, int n)
         int n, lu, chol;
     };
     static const Row rows[] = {{0, 16, 16}, {512, 16, 16}, {1024, 16, 16}, {2048, 16, 16}, {4096, 16, 16},
-                               {8192, 128, 16}};
+                               {8192, 128, 24}};
     int nb = 16;
     for (const Row &r : rows)
         if (n >= r.n)
