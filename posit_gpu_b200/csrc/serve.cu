@@ -1,6 +1,7 @@
 // serve.cu -- the request loop for served Ax = b solves (include/posit_gpu.h).
 //
-// One loop thread admits queued requests in arrival order while the admitted but
+// One loop thread admits queued requests (arrival order by windows of order_window_ms,
+// largest work first within a window) while the admitted but
 // unfinished requests stay under `max_inflight` and their device bytes (matrix or
 // factor, right-hand sides, workspace) under the memory budget; when the budget is
 // short it first evicts idle cached factors, least recently used first.  Admitted
@@ -113,6 +114,7 @@ struct posit_server {
     // configuration
     size_t budget = 0;
     int max_inflight = 0, max_queue = 0, batch_max_n = 0, nb = 0;
+    double order_window_ms = 50.0;
     bool cache_on = true;
     int device = 0, sms = 148;
     cudaMemPool_t pool = nullptr;
@@ -132,6 +134,7 @@ struct posit_server {
     std::atomic<long long> queued{0};
 
     // loop thread only
+    Clock::time_point t_created = Clock::now(); // origin of the admission-order windows
     std::deque<Req> pending;
     std::unordered_map<long long, Factor *> cache;
     size_t used = 0;
@@ -480,9 +483,36 @@ void finish_unit(posit_server *s, Unit *u, std::vector<Req> &done)
     delete u;
 }
 
-// One admission pass over the queue, in arrival order (loop thread).
+// Admission order.  Requests submitted within one order window (order_window_ms) are taken
+// largest estimated work first (factorization n^3, solve n^2 * nrhs); the windows
+// themselves go first come, first served.  In a burst this starts the long solves at once
+// instead of after the queue ahead of them, which is what ends the burst sooner; at
+// arrival rates where a window holds one request the order is arrival order.
+double est_work(const Req &r)
+{
+    const double n = r->q.n;
+    const double fact = r->q.kind == POSIT_BATCH_LU ? 2.0 / 3.0 : 1.0 / 3.0;
+    return fact * n * n * n + 2.0 * n * n * r->q.nrhs;
+}
+
+void order_pending(posit_server *s)
+{
+    if (s->pending.size() < 2)
+        return;
+    const Clock::time_point t0 = s->t_created;
+    std::stable_sort(s->pending.begin(), s->pending.end(), [&](const Req &a, const Req &b) {
+        const long wa = (long)(ms_between(t0, a->t_submit) / s->order_window_ms);
+        const long wb = (long)(ms_between(t0, b->t_submit) / s->order_window_ms);
+        if (wa != wb)
+            return wa < wb;
+        return est_work(a) > est_work(b);
+    });
+}
+
+// One admission pass over the queue, in admission order (loop thread).
 void admit(posit_server *s, std::vector<Req> &done, std::vector<Unit *> &units)
 {
+    order_pending(s);
     // Lanes reserved for batched units keep small requests from waiting behind long
     // blocked ones; a batched unit may also take a free blocked lane.
     std::vector<Lane *> idle_batch, idle_blocked;
@@ -718,6 +748,7 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
     s->max_queue = c.max_queue > 0 ? c.max_queue : (1 << 20);
     s->batch_max_n = c.batch_max_n > 0 ? std::min(c.batch_max_n, POSIT_BATCH_MAX_N) : 256;
     s->nb = c.nb > 0 ? c.nb : 0; // 0: the tuned width for each request's n
+    s->order_window_ms = c.order_window_ms > 0 ? (double)c.order_window_ms : 50.0;
     s->cache_on = c.cache_off == 0;
     const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 64);
     const int nbatch = std::min(nlanes - 1, c.batch_lanes > 0 ? c.batch_lanes : 4);

@@ -205,3 +205,25 @@ def test_cancel_bad_arguments_and_shutdown(cuda_ok):
     for _ in range(3):
         srv.submit(0, 300, 2, _problem(rng, 0, 300), _rhs(rng, 300, 2), np.zeros(600, np.uint32))
     srv.close()
+
+
+def test_burst_admits_largest_work_first(cuda_ok):
+    """Requests submitted within one order window are admitted largest work first: behind a
+    request that holds the only slot, four more of different n are admitted by decreasing
+    n, whatever their submission order, and each result still equals the per-call one."""
+    import posit_gpu_b200 as pg
+    rng = np.random.default_rng(21)
+    with pg.Server(max_inflight=1, lanes=2, batch_max_n=64, order_window_ms=60000) as srv:
+        A0, B0 = _problem(rng, 0, 1500), _rhs(rng, 1500, 1)
+        t0 = srv.submit(0, 1500, 1, A0, B0, np.zeros_like(B0))
+        sizes = [300, 900, 400, 600]
+        probs = [(_problem(rng, 0, n), _rhs(rng, n, 1)) for n in sizes]
+        outs = [np.zeros_like(b) for _, b in probs]
+        ts = [srv.submit(0, n, 1, a, b, x) for n, (a, b), x in zip(sizes, probs, outs)]
+        assert srv.wait(t0)["status"] == 0
+        res = [srv.wait(t) for t in ts]
+        assert all(r["status"] == 0 for r in res)
+        admitted = sorted(range(4), key=lambda i: res[i]["queue_ms"])
+        assert [sizes[i] for i in admitted] == [900, 600, 400, 300]
+        for n, (a, b), x in zip(sizes, probs, outs):
+            assert np.array_equal(x, _per_call(pg, 0, n, 1, a, b)[0])
