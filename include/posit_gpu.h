@@ -163,8 +163,9 @@ void posit_batch_plan_destroy(posit_batch_plan *plan);
 
 /* ---- Served solves (no reference counterpart) ---------------------------------------
  * A request loop for Ax = b solves of mixed kind, n and nrhs that arrive over time.  A
- * loop thread admits queued requests -- windows of order_window_ms in arrival order, the
- * largest work first within a window -- while admitted-but-unfinished
+ * loop thread admits queued requests in arrival order (with order_window_ms > 0: windows of
+ * that many ms in arrival order, the largest work first within a window) while
+ * admitted-but-unfinished
  * requests stay under max_inflight and their device bytes (matrix/factor, right-hand
  * sides, workspace) under the memory budget, evicting idle cached factors (least
  * recently used first) when it is short; a request that finds no free lane of its kind
@@ -201,8 +202,8 @@ typedef struct {
     int nb;               /* panel width of the blocked path; 0 = the tuned width for each n */
     int cache_off;        /* 1: never keep factors */
     int batch_lanes;      /* lanes reserved for batched units; 0 = 4 */
-    int order_window_ms;  /* requests submitted within one window of this many ms are admitted
-                             largest work first, windows in arrival order; 0 = 50 */
+    int order_window_ms;  /* > 0: requests submitted within one window of this many ms are
+                             admitted largest work first, windows in arrival order; 0 = arrival order */
 } posit_server_config;
 typedef struct {
     int kind;             /* POSIT_BATCH_LU or POSIT_BATCH_CHOLESKY (lower) */

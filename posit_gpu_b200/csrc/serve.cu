@@ -1,7 +1,7 @@
 // serve.cu -- the request loop for served Ax = b solves (include/posit_gpu.h).
 //
-// One loop thread admits queued requests (arrival order by windows of order_window_ms,
-// largest work first within a window) while the admitted but
+// One loop thread admits queued requests in arrival order (optionally largest work first
+// within windows of order_window_ms) while the admitted but
 // unfinished requests stay under `max_inflight` and their device bytes (matrix or
 // factor, right-hand sides, workspace) under the memory budget; when the budget is
 // short it first evicts idle cached factors, least recently used first.  Admitted
@@ -114,7 +114,7 @@ struct posit_server {
     // configuration
     size_t budget = 0;
     int max_inflight = 0, max_queue = 0, batch_max_n = 0, nb = 0;
-    double order_window_ms = 50.0;
+    double order_window_ms = 0.0; // 0: arrival order
     bool cache_on = true;
     int device = 0, sms = 148;
     cudaMemPool_t pool = nullptr;
@@ -483,11 +483,12 @@ void finish_unit(posit_server *s, Unit *u, std::vector<Req> &done)
     delete u;
 }
 
-// Admission order.  Requests submitted within one order window (order_window_ms) are taken
-// largest estimated work first (factorization n^3, solve n^2 * nrhs); the windows
-// themselves go first come, first served.  In a burst this starts the long solves at once
-// instead of after the queue ahead of them, which is what ends the burst sooner; at
-// arrival rates where a window holds one request the order is arrival order.
+// Admission order: arrival order by default.  With order_window_ms > 0, requests submitted
+// within one such window are taken largest estimated work first (factorization n^3, solve
+// n^2 * nrhs), the windows themselves first come, first served: a makespan-oriented order
+// for batch jobs.  (Measured on the serving burst it starts the long solves at once but
+// gains no throughput -- the burst is bound by the GPU's work, not by the order -- and
+// raises the median latency, so it is not the default.)
 double est_work(const Req &r)
 {
     const double n = r->q.n;
@@ -497,7 +498,7 @@ double est_work(const Req &r)
 
 void order_pending(posit_server *s)
 {
-    if (s->pending.size() < 2)
+    if (s->order_window_ms <= 0.0 || s->pending.size() < 2)
         return;
     const Clock::time_point t0 = s->t_created;
     std::stable_sort(s->pending.begin(), s->pending.end(), [&](const Req &a, const Req &b) {
@@ -748,7 +749,7 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
     s->max_queue = c.max_queue > 0 ? c.max_queue : (1 << 20);
     s->batch_max_n = c.batch_max_n > 0 ? std::min(c.batch_max_n, POSIT_BATCH_MAX_N) : 256;
     s->nb = c.nb > 0 ? c.nb : 0; // 0: the tuned width for each request's n
-    s->order_window_ms = c.order_window_ms > 0 ? (double)c.order_window_ms : 50.0;
+    s->order_window_ms = c.order_window_ms > 0 ? (double)c.order_window_ms : 0.0;
     s->cache_on = c.cache_off == 0;
     const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 64);
     const int nbatch = std::min(nlanes - 1, c.batch_lanes > 0 ? c.batch_lanes : 4);
