@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--batch-max-n", type=int, default=0, help="serve: batched-kernel size limit (0: default)")
     ap.add_argument("--lanes", type=int, default=0, help="serve: CUDA streams of the server (0: default)")
     ap.add_argument("--launch-threads", type=int, default=0, help="serve: launcher threads (0: default)")
+    ap.add_argument("--profile-path", default="", choices=["", "percall", "served"],
+                    help="serve: bracket only this path with cudaProfilerStart/Stop (for ncu "
+                         "--profile-from-start off); both paths still run")
     return ap.parse_args()
 
 
@@ -765,6 +768,8 @@ def serve_arm(args):
     fac_src = {m: mats[m].numpy().view(np.uint32).copy() for (_, _, _, m) in reqs[:S]}
     xs = [rhs[i].numpy().view(np.uint32).copy() for i in range(S)]
     pc_info, factors, pc_lat = [], {}, []
+    if args.profile_path == "percall":
+        torch.cuda.profiler.start()
     t0 = time.perf_counter()
     for i in range(S):
         kind, n, r, m = reqs[i]
@@ -782,6 +787,8 @@ def serve_arm(args):
         pc_info.append(info)
         pc_lat.append((time.perf_counter() - ts) * 1e3)
     pc_s = time.perf_counter() - t0
+    if args.profile_path == "percall":
+        torch.cuda.profiler.stop()
     pc_rate = S / pc_s
 
     # served, at each arrival rate
@@ -790,6 +797,8 @@ def serve_arm(args):
     same_across = True
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
+    if args.profile_path == "served":
+        torch.cuda.profiler.start()
     for rate in rates:
         outs = [zeros(i) for i in range(R)]
         arng = np.random.default_rng(77)
@@ -844,6 +853,8 @@ def serve_arm(args):
                      "evictions": st["evictions"], "bytes_peak_gb": round(st["bytes_peak"] / 1e9, 2),
                      "bit_identical_to_per_call_on_sample": bool(same_pc), "mismatches": mismatches,
                      "slowest": slowest})
+    if args.profile_path == "served":
+        torch.cuda.profiler.stop()
     clocks = sampler.stop()
     repeats = sum(1 for i, q in enumerate(reqs) if q[3] != i)
     best = max(runs, key=lambda x: x["solves_per_s"])
