@@ -370,227 +370,6 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
     }
 }
 
-// ---------------------------------------------------------------------------
-// Small panels (at most 1024 rows, SMALL_JB columns) in registers.
-// ---------------------------------------------------------------------------
-// One CTA of 1024 threads; thread t holds row t of the panel in SMALL_JB FP64 registers
-// for the whole panel.  The rounding constants come from the shared-memory table the GEMM
-// uses (F64ConstTable8).  Per column of LU: the pivot search (warp shuffles, then warp 0
-// over the warps), the pivot decision (thread 0), the rows of k and p written to shared
-// memory, and after a barrier threads k and p take each other's row while every thread
-// reads the pivot row as -u_kc; then each thread scales and updates its own row.  Same
-// per-element operations and order as the other panel forms.
-constexpr int SMALL_JB = 16;
-constexpr int SMALL_THREADS = 1024;
-
-__device__ __forceinline__ double mac_tab(double c, double t, double a, F64ConstTable8 cof)
-{
-    bool bad;
-    const double r = f64_posit_mac(c, t, a, cof, bad);
-    return bad ? f64_posit_mac_exact(c, t, a) : r;
-}
-
-// a[k] for a run-time k with a[] kept in registers (a select per entry, no local memory)
-template <int N>
-__device__ __forceinline__ double reg_get(const double (&a)[N], int k)
-{
-    double v = a[0];
-#pragma unroll
-    for (int c = 1; c < N; ++c)
-        v = (c == k) ? a[c] : v;
-    return v;
-}
-template <int N>
-__device__ __forceinline__ void reg_set(double (&a)[N], int k, double v)
-{
-#pragma unroll
-    for (int c = 0; c < N; ++c)
-        a[c] = (c == k) ? v : a[c];
-}
-
-__device__ __forceinline__ void fill_const_table(double *tab, int tid, int nthreads)
-{
-    for (int i = tid; i < F64_CONST_ENTRIES; i += nthreads)
-        tab[i] = f64_from_hi(f64_round_const_top(i));
-}
-
-__global__ void __launch_bounds__(SMALL_THREADS) lu_panel_small_kernel(uint32_t *__restrict__ P, size_t lda, int M,
-                                                                       int row0, int *__restrict__ ipiv,
-                                                                       int *__restrict__ info)
-{
-    __shared__ double s_tab[F64_CONST_ENTRIES];
-    __shared__ double s_key[32];
-    __shared__ int s_idx[32];
-    __shared__ double s_rowk[SMALL_JB], s_rowp[SMALL_JB];
-    __shared__ PivotInfo s_pi;
-    if (*info < 0)
-        return;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    fill_const_table(s_tab, t, SMALL_THREADS);
-    const F64ConstTable8 cof{s_tab};
-    double a[SMALL_JB];
-    const bool mine = t < M;
-#pragma unroll
-    for (int c = 0; c < SMALL_JB; ++c)
-        a[c] = mine ? p32_to_double(P[t + (size_t)c * lda]) : 0.0;
-    __syncthreads();
-#pragma unroll 1
-    for (int k = 0; k < SMALL_JB; ++k) {
-        // iRamax over rows [k, M) (iRamax.cpp:65-71): larger key wins, equal keys the lower row
-        double best = (mine && t >= k) ? pivot_key(reg_get(a, k)) : -2.0;
-        int bidx = (mine && t >= k) ? t : -1;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
-            const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
-            if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
-                best = k2;
-                bidx = i2;
-            }
-        }
-        if (lane == 0) {
-            s_key[warp] = best;
-            s_idx[warp] = bidx;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            best = s_key[lane];
-            bidx = s_idx[lane];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
-                const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
-                if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
-                    best = k2;
-                    bidx = i2;
-                }
-            }
-            if (lane == 0)
-                s_pi.row = bidx;
-        }
-        __syncthreads();
-        const int p = s_pi.row;
-        if (t == p) {
-#pragma unroll
-            for (int c = 0; c < SMALL_JB; ++c)
-                s_rowp[c] = a[c];
-        }
-        if (t == k) {
-#pragma unroll
-            for (int c = 0; c < SMALL_JB; ++c)
-                s_rowk[c] = a[c];
-        }
-        if (t == p) { // the pivot decision, from the pivot row's own value
-            const uint32_t piv = p32_from_double_exact(reg_get(a, k));
-            PivotInfo pi;
-            pi.row = p;
-            pi.piv = piv;
-            if (piv == 0) {
-                pi.mode = 0;
-                pi.recip = 0;
-                if (*info == 0)
-                    *info = row0 + k + 1;
-            } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
-                pi.mode = 1;
-                pi.recip = pdiv(P32_ONE, piv);
-            } else {
-                pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
-                pi.recip = 0;
-            }
-            ipiv[row0 + k] = row0 + p + 1; // 1-based, global
-            s_pi = pi;
-        }
-        __syncthreads();
-        const PivotInfo pi = s_pi;
-        if (pi.piv != 0 && p != k) { // Rgetrf2.cpp:107-117: rows k and p change places
-            if (t == k) {
-#pragma unroll
-                for (int c = 0; c < SMALL_JB; ++c)
-                    a[c] = s_rowp[c];
-            } else if (t == p) {
-#pragma unroll
-                for (int c = 0; c < SMALL_JB; ++c)
-                    a[c] = s_rowk[c];
-            }
-        }
-        // the new row k: the pivot row, or row k itself when nothing moved
-        const double *uk = (pi.piv != 0) ? s_rowp : s_rowk;
-        if (mine && t > k) {
-            const double dl = p32_to_double(lu_scaled(p32_from_double_exact(reg_get(a, k)), pi));
-            reg_set(a, k, dl);
-#pragma unroll
-            for (int c = 1; c < SMALL_JB; ++c) // a_ic + (-u_kc)*l_i in the FP64 step, c > k
-                if (c > k)
-                    a[c] = mac_tab(a[c], -uk[c], dl, cof);
-        }
-        __syncthreads(); // s_rowk / s_rowp / s_key are rewritten by the next column
-    }
-    if (mine) {
-#pragma unroll
-        for (int c = 0; c < SMALL_JB; ++c)
-            P[t + (size_t)c * lda] = p32_from_double_exact(a[c]);
-    }
-}
-
-// Lower Cholesky, the same way: thread k takes the square root and reciprocal of its own
-// a_kk, threads below scale their entry of column k, the panel rows' -l_ck go through
-// shared memory, each thread updates its own row (Rpotrf2.cpp:90-97, Rtrsm.cpp:265-268).
-__global__ void __launch_bounds__(SMALL_THREADS) chol_panel_small_kernel(uint32_t *__restrict__ P, size_t lda,
-                                                                         int M, int row0, int *__restrict__ info)
-{
-    __shared__ double s_tab[F64_CONST_ENTRIES];
-    __shared__ double s_l[SMALL_JB];
-    __shared__ uint32_t s_recip;
-    __shared__ int s_stop;
-    if (*info != 0)
-        return;
-    const int t = threadIdx.x;
-    fill_const_table(s_tab, t, SMALL_THREADS);
-    const F64ConstTable8 cof{s_tab};
-    double a[SMALL_JB];
-    const bool mine = t < M;
-#pragma unroll
-    for (int c = 0; c < SMALL_JB; ++c)
-        a[c] = mine ? p32_to_double(P[t + (size_t)c * lda]) : 0.0;
-#pragma unroll 1
-    for (int k = 0; k < SMALL_JB; ++k) {
-        if (t == k) {
-            const uint32_t akk = p32_from_double_exact(reg_get(a, k));
-            s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
-            if (s_stop) {
-                *info = row0 + k + 1;
-            } else {
-                const uint32_t lkk = psqrt(akk);
-                s_recip = pdiv(P32_ONE, lkk);
-                reg_set(a, k, p32_to_double(lkk));
-            }
-        }
-        __syncthreads();
-        if (s_stop)
-            break;
-        double dl = 0.0;
-        if (mine && t > k) {
-            dl = p32_to_double(pmul(s_recip, p32_from_double_exact(reg_get(a, k))));
-            reg_set(a, k, dl);
-            if (t < SMALL_JB)
-                s_l[t] = -dl;
-        }
-        __syncthreads();
-        if (mine && t > k) {
-#pragma unroll
-            for (int c = 1; c < SMALL_JB; ++c) // a_ic + (-l_ck)*l_i in the FP64 step, k < c <= i
-                if (c > k && c <= t)
-                    a[c] = mac_tab(a[c], s_l[c], dl, cof);
-        }
-        __syncthreads(); // s_l, s_stop and s_recip are rewritten by the next column
-    }
-    if (mine) {
-#pragma unroll
-        for (int c = 0; c < SMALL_JB; ++c)
-            P[t + (size_t)c * lda] = p32_from_double_exact(a[c]);
-    }
-}
-
 // After a panel of columns [j, j+jb) (jb <= ROWS_JB_MAX): the panel's row interchanges
 // (Rlaswp, Rlaswp.cpp:77-107, in ascending order) on every column outside the panel, and
 // the unit-lower solve of the U12 block (Rtrsm('L', 'L', 'N', 'U'), Rtrsm.cpp:139-154, zero
@@ -600,12 +379,9 @@ __global__ void __launch_bounds__(SMALL_THREADS) chol_panel_small_kernel(uint32_
 constexpr int ROWS_JB_MAX = 32;
 constexpr int ROWS_THREADS = 128;
 
-// JB > 0: the panel width is JB (arrays in registers); JB == 0: jb <= ROWS_JB_MAX at run time.
-template <int JB>
 __global__ void __launch_bounds__(ROWS_THREADS) lu_rows_kernel(uint32_t *__restrict__ A, size_t lda, int n, int j,
-                                                               int jb_rt, const int *__restrict__ ipiv)
+                                                               int jb, const int *__restrict__ ipiv)
 {
-    const int jb = JB > 0 ? JB : jb_rt;
     __shared__ double s_L[ROWS_JB_MAX * ROWS_JB_MAX]; // l_ik at [i * ROWS_JB_MAX + k], FP64
     __shared__ int s_t[ROWS_JB_MAX];                  // interchange i: row j+i <-> row s_t[i] (0-based)
     __shared__ int s_alias[ROWS_JB_MAX];              // below the block: the first interchange with that row
@@ -635,70 +411,41 @@ __global__ void __launch_bounds__(ROWS_THREADS) lu_rows_kernel(uint32_t *__restr
         return;
     const int c = ci < j ? ci : ci + jb; // the columns outside the panel
     uint32_t *col = A + (size_t)c * lda;
-    constexpr int N = JB > 0 ? JB : ROWS_JB_MAX;
-    uint32_t v[N], w[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-        if (i < jb)
-            v[i] = col[j + i];
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-        if (i < jb && s_alias[i] == i)
+    uint32_t v[ROWS_JB_MAX], w[ROWS_JB_MAX];
+    for (int i = 0; i < jb; ++i)
+        v[i] = col[j + i];
+    for (int i = 0; i < jb; ++i)
+        if (s_alias[i] == i)
             w[i] = col[s_t[i]];
-    // the interchanges in order: v[i] <-> v[t - j] (t in the block) or <-> w[alias] (below
-    // it); selects over the arrays keep them in registers when JB is known
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        if (i >= jb)
-            break;
+    for (int i = 0; i < jb; ++i) {
         const int t = s_t[i];
         if (t == j + i)
             continue;
-        const bool in = t < j + jb;
-        const int o = in ? t - j : s_alias[i];
-        uint32_t other = 0;
-#pragma unroll
-        for (int q = 0; q < N; ++q)
-            other = (q == o) ? (in ? v[q] : w[q]) : other;
+        uint32_t *o = t < j + jb ? &v[t - j] : &w[s_alias[i]];
         const uint32_t x = v[i];
-#pragma unroll
-        for (int q = 0; q < N; ++q) {
-            if (q == o && in)
-                v[q] = x;
-            if (q == o && !in)
-                w[q] = x;
-        }
-        v[i] = other;
+        v[i] = *o;
+        *o = x;
     }
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-        if (i < jb && s_alias[i] == i)
+    for (int i = 0; i < jb; ++i)
+        if (s_alias[i] == i)
             col[s_t[i]] = w[i];
     if (c > j) { // U12 <- L11^-1 A12, column-oriented as Rtrsm.cpp:139-154 (unit diagonal)
-        double x[N];
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-            x[i] = i < jb ? p32_to_double(v[i]) : 0.0;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
+        double x[ROWS_JB_MAX];
+        for (int i = 0; i < jb; ++i)
+            x[i] = p32_to_double(v[i]);
+        for (int k = 0; k < jb; ++k) {
             const double bk = x[k];
-            if (k < jb && bk != 0.0) {
+            if (bk != 0.0) {
                 const double nbk = -bk;
-#pragma unroll
-                for (int i = k + 1; i < N; ++i)
-                    if (i < jb)
-                        x[i] = f64_posit_mac_checked(x[i], nbk, s_L[i * ROWS_JB_MAX + k]);
+                for (int i = k + 1; i < jb; ++i)
+                    x[i] = f64_posit_mac_checked(x[i], nbk, s_L[i * ROWS_JB_MAX + k]);
             }
         }
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-            if (i < jb)
-                v[i] = p32_from_double(x[i]);
+        for (int i = 0; i < jb; ++i)
+            v[i] = p32_from_double(x[i]);
     }
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-        if (i < jb)
-            col[j + i] = v[i];
+    for (int i = 0; i < jb; ++i)
+        col[j + i] = v[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -1632,9 +1379,7 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j; // indexed by panel-local row
         const PanelForm pf = panel_form(M, jb);
-        if (jb == SMALL_JB && M <= SMALL_THREADS) {
-            lu_panel_small_kernel<<<1, SMALL_THREADS, 0, st>>>(P, L, M, j, ipiv, info);
-        } else if (pf.ncta > 0) {
+        if (pf.ncta > 0) {
             cudaError_t e = launch_panel_cluster(lu_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, ipiv, info);
             if (e != cudaSuccess)
                 return e;
@@ -1647,13 +1392,8 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         }
         if (jb <= ROWS_JB_MAX) {
             if (n > jb)
-            {
-                const int grid = (n - jb + ROWS_THREADS - 1) / ROWS_THREADS;
-                if (jb == 16)
-                    lu_rows_kernel<16><<<grid, ROWS_THREADS, 0, st>>>(A, L, n, j, jb, ipiv);
-                else
-                    lu_rows_kernel<0><<<grid, ROWS_THREADS, 0, st>>>(A, L, n, j, jb, ipiv);
-            }
+                lu_rows_kernel<<<(n - jb + ROWS_THREADS - 1) / ROWS_THREADS, ROWS_THREADS, 0, st>>>(A, L, n, j, jb,
+                                                                                                 ipiv);
         } else {
             if (j > 0)
                 laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
@@ -1705,9 +1445,7 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j;
         const PanelForm pf = panel_form(M, jb);
-        if (jb == SMALL_JB && M <= SMALL_THREADS) {
-            chol_panel_small_kernel<<<1, SMALL_THREADS, 0, st>>>(P, L, M, j, info);
-        } else if (pf.ncta > 0) {
+        if (pf.ncta > 0) {
             cudaError_t e = launch_panel_cluster(chol_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, info);
             if (e != cudaSuccess)
                 return e;
