@@ -373,19 +373,21 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
 // After a panel of columns [j, j+jb) (jb <= ROWS_JB_MAX): the panel's row interchanges
 // (Rlaswp, Rlaswp.cpp:77-107, in ascending order) on every column outside the panel, and
 // the unit-lower solve of the U12 block (Rtrsm('L', 'L', 'N', 'U'), Rtrsm.cpp:139-154, zero
-// multipliers skipped as there) on the columns right of it, in one launch: one thread per
-// column, its rows j..j+jb-1 and the interchanges' other rows held in registers (loaded
-// together, so one memory latency per column instead of one per interchange).
+// multipliers skipped as there) on the columns right of it, in one launch: one warp per
+// column, lane i holding row j+i and (for an interchange with a row below the block) that
+// row's value, loaded together; the interchanges run in order as exchanges between lanes,
+// the solve as jb steps of one multiply-add per lane with the step's b_k from its lane.
 constexpr int ROWS_JB_MAX = 32;
-constexpr int ROWS_THREADS = 128;
+constexpr int ROWS_THREADS = 256; // 8 columns per block
 
 __global__ void __launch_bounds__(ROWS_THREADS) lu_rows_kernel(uint32_t *__restrict__ A, size_t lda, int n, int j,
                                                                int jb, const int *__restrict__ ipiv)
 {
+    constexpr unsigned FULL = 0xFFFFFFFFu;
     __shared__ double s_L[ROWS_JB_MAX * ROWS_JB_MAX]; // l_ik at [i * ROWS_JB_MAX + k], FP64
     __shared__ int s_t[ROWS_JB_MAX];                  // interchange i: row j+i <-> row s_t[i] (0-based)
     __shared__ int s_alias[ROWS_JB_MAX];              // below the block: the first interchange with that row
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     for (int e = tid; e < jb * jb; e += ROWS_THREADS) {
         const int i = e % jb, k = e / jb;
         s_L[i * ROWS_JB_MAX + k] = p32_to_double(A[(j + i) + (size_t)(j + k) * lda]);
@@ -406,46 +408,45 @@ __global__ void __launch_bounds__(ROWS_THREADS) lu_rows_kernel(uint32_t *__restr
         s_alias[i] = a;
     }
     __syncthreads();
-    const int ci = blockIdx.x * ROWS_THREADS + tid;
+    const int ci = blockIdx.x * (ROWS_THREADS / 32) + (tid >> 5);
     if (ci >= n - jb)
-        return;
+        return; // the whole warp
     const int c = ci < j ? ci : ci + jb; // the columns outside the panel
     uint32_t *col = A + (size_t)c * lda;
-    uint32_t v[ROWS_JB_MAX], w[ROWS_JB_MAX];
-    for (int i = 0; i < jb; ++i)
-        v[i] = col[j + i];
-    for (int i = 0; i < jb; ++i)
-        if (s_alias[i] == i)
-            w[i] = col[s_t[i]];
+    const bool row = lane < jb;
+    const int my_t = row ? s_t[lane] : 0, my_alias = row ? s_alias[lane] : -1;
+    uint32_t v = row ? col[j + lane] : 0u;               // row j+lane
+    uint32_t w = (my_alias == lane) ? col[my_t] : 0u;  // row my_t (below the block)
     for (int i = 0; i < jb; ++i) {
         const int t = s_t[i];
         if (t == j + i)
             continue;
-        uint32_t *o = t < j + jb ? &v[t - j] : &w[s_alias[i]];
-        const uint32_t x = v[i];
-        v[i] = *o;
-        *o = x;
-    }
-    for (int i = 0; i < jb; ++i)
-        if (s_alias[i] == i)
-            col[s_t[i]] = w[i];
-    if (c > j) { // U12 <- L11^-1 A12, column-oriented as Rtrsm.cpp:139-154 (unit diagonal)
-        double x[ROWS_JB_MAX];
-        for (int i = 0; i < jb; ++i)
-            x[i] = p32_to_double(v[i]);
-        for (int k = 0; k < jb; ++k) {
-            const double bk = x[k];
-            if (bk != 0.0) {
-                const double nbk = -bk;
-                for (int i = k + 1; i < jb; ++i)
-                    x[i] = f64_posit_mac_checked(x[i], nbk, s_L[i * ROWS_JB_MAX + k]);
-            }
+        const bool in = t < j + jb;
+        const int o = in ? t - j : s_alias[i];
+        const uint32_t vi = __shfl_sync(FULL, v, i);
+        const uint32_t vo = __shfl_sync(FULL, in ? v : w, o);
+        if (lane == o) {
+            if (in)
+                v = vi;
+            else
+                w = vi;
         }
-        for (int i = 0; i < jb; ++i)
-            v[i] = p32_from_double(x[i]);
+        if (lane == i)
+            v = vo;
     }
-    for (int i = 0; i < jb; ++i)
-        col[j + i] = v[i];
+    if (my_alias == lane)
+        col[my_t] = w;
+    if (c > j) { // U12 <- L11^-1 A12, column-oriented as Rtrsm.cpp:139-154 (unit diagonal)
+        double x = row ? p32_to_double(v) : 0.0;
+        for (int k = 0; k < jb; ++k) {
+            const double bk = __shfl_sync(FULL, x, k);
+            if (bk != 0.0 && lane > k && row)
+                x = f64_posit_mac_checked(x, -bk, s_L[lane * ROWS_JB_MAX + k]);
+        }
+        v = p32_from_double(x);
+    }
+    if (row)
+        col[j + lane] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -1392,8 +1393,8 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         }
         if (jb <= ROWS_JB_MAX) {
             if (n > jb)
-                lu_rows_kernel<<<(n - jb + ROWS_THREADS - 1) / ROWS_THREADS, ROWS_THREADS, 0, st>>>(A, L, n, j, jb,
-                                                                                                 ipiv);
+                lu_rows_kernel<<<(n - jb + ROWS_THREADS / 32 - 1) / (ROWS_THREADS / 32), ROWS_THREADS, 0, st>>>(
+                    A, L, n, j, jb, ipiv);
         } else {
             if (j > 0)
                 laswp_kernel<<<(j + 127) / 128, 128, 0, st>>>(A, L, j, j + 1, j + jb, ipiv, 1, info);
