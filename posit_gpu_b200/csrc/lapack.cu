@@ -292,9 +292,10 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
                     s_val[warp] = bval;
                 }
                 __syncthreads();
-                best = s_key[lane];
-                bidx = s_idx[lane];
-                bval = s_val[lane];
+                const bool slot = lane < (int)(blockDim.x >> 5); // one slot per warp of the block
+                best = slot ? s_key[lane] : -2.0;
+                bidx = slot ? s_idx[lane] : -1;
+                bval = slot ? s_val[lane] : 0.0;
             }
         }
         if (tid == 0) {
