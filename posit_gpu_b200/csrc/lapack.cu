@@ -246,9 +246,13 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
     __shared__ int s_cidx;            // the whole cluster
     __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row
     __shared__ PivotInfo s_pi;
+    __shared__ uint32_t s_tab[F64_CONST_ENTRIES]; // rounding constants (F64ConstTable)
     if (*info < 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < F64_CONST_ENTRIES; i += PANEL1_THREADS)
+        s_tab[i] = f64_round_const_top(i);
+    const F64ConstTable cof{s_tab}; // read only after the first barrier below
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
     auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
     for (int r = 0; r < R; ++r) {
@@ -351,14 +355,19 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
         for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
             s_u[c] = -*panel_entry(cluster, s_rows, jb, G, k, c);
         __syncthreads();
+        const double drecip = p32_to_double(pi.recip);
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i > k && i < M) {
-                const uint32_t l = lu_scaled(p32_from_double_exact(own(r, k)), pi);
-                const double dl = p32_to_double(l);
-                own(r, k) = dl;
+                double *row = &own(r, 0);
+                // Rscal (x*recip, the FP64 product step) or the element-wise division
+                const double dl = pi.mode == 1 ? f64_posit_mul_checked(row[(size_t)k * PANEL1_THREADS], drecip, cof)
+                                               : p32_to_double(lu_scaled(
+                                                     p32_from_double_exact(row[(size_t)k * PANEL1_THREADS]), pi));
+                row[(size_t)k * PANEL1_THREADS] = dl;
                 for (int c = k + 1; c < jb; ++c) // a_ic + (-u_kc)*l_i in the FP64 step
-                    own(r, c) = f64_posit_mac_checked(own(r, c), s_u[c], dl);
+                    row[(size_t)c * PANEL1_THREADS] =
+                        f64_posit_mac_checked(row[(size_t)c * PANEL1_THREADS], s_u[c], dl, cof);
             }
         }
     }
@@ -1118,9 +1127,13 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
     __shared__ double s_l[PANEL1_MAX_JB];           // -l_ck of the current column
     __shared__ uint32_t s_recip, s_lkk;
     __shared__ int s_stop;
+    __shared__ uint32_t s_tab[F64_CONST_ENTRIES]; // rounding constants (F64ConstTable)
     if (*info != 0) // written only by earlier launches: the same in every CTA
         return;
     const int tid = threadIdx.x;
+    for (int i = tid; i < F64_CONST_ENTRIES; i += PANEL1_THREADS)
+        s_tab[i] = f64_round_const_top(i);
+    const F64ConstTable cof{s_tab}; // read only after the first barrier below
     const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
     auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
     for (int r = 0; r < R; ++r) {
@@ -1145,11 +1158,11 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
         __syncthreads();
         if (s_stop) // decided from the same a_kk in every CTA
             break;
-        const uint32_t recip = s_recip;
+        const double drecip = p32_to_double(s_recip);
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
-            if (i > k && i < M)
-                own(r, k) = p32_to_double(pmul(recip, p32_from_double_exact(own(r, k))));
+            if (i > k && i < M) // (1/l_kk)*a_ik, the FP64 product step
+                own(r, k) = f64_posit_mul_checked(own(r, k), drecip, cof);
         }
         panel_sync(cluster, ncta); // the scaled column is visible, and every CTA has read a_kk
         if (rank == 0 && tid == 0)
@@ -1160,10 +1173,12 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
         for (int r = 0; r < R; ++r) {
             const int i = g + r * G;
             if (i > k && i < M) {
-                const double dl = own(r, k);
+                double *row = &own(r, 0);
+                const double dl = row[(size_t)k * PANEL1_THREADS];
                 const int cend = min(jb - 1, i);
                 for (int c = k + 1; c <= cend; ++c) // a_ic + (-l_ck)*l_i in the FP64 step
-                    own(r, c) = f64_posit_mac_checked(own(r, c), s_l[c], dl);
+                    row[(size_t)c * PANEL1_THREADS] =
+                        f64_posit_mac_checked(row[(size_t)c * PANEL1_THREADS], s_l[c], dl, cof);
             }
         }
     }

@@ -710,6 +710,27 @@ PG_HD double f64_posit_mac_checked(double c, double t, double a)
     return fail ? f64_posit_mac_exact(c, t, a) : r;
 }
 
+// The same with the constants from a table.
+template <class ConstOf>
+PG_HD double f64_posit_mac_checked(double c, double t, double a, ConstOf const_of)
+{
+    bool fail;
+    const double r = f64_posit_mac(c, t, a, const_of, fail);
+    return fail ? f64_posit_mac_exact(c, t, a) : r;
+}
+
+// x*y rounded as p32_mul (kernel_entry.cl:399-538) rounds it, both posit32 values held in
+// FP64: the exact product rounded once onto the posit grid of its binade, fma(x, y, Cp) - Cp
+// (the product step of f64_posit_mac).  A product outside the fast window (its constant is
+// NaN) and NaR operands (NaN) go through the pattern routine.
+template <class ConstOf>
+PG_HD double f64_posit_mul_checked(double x, double y, ConstOf const_of)
+{
+    const double Cp = const_of(f64_mul(x, y));
+    const double q = f64_add(f64_fma(x, y, Cp), -Cp);
+    return q == q ? q : p32_to_double(pmul(p32_from_double(x), p32_from_double(y)));
+}
+
 // FP64 -> posit32 for a value that IS a posit32 value (an output of the FP64 steps or of
 // p32_to_double): the fields are assembled without rounding.  Regimes longer than 27 bits
 // (fewer than one fraction bit) and NaN go through p32_from_double.
