@@ -655,99 +655,10 @@ __global__ void __launch_bounds__(32) trsm_llt_kernel(const uint32_t *__restrict
         bcol[i] = s_col[i];
 }
 
-// The same solve split over warps (one block per right-hand side, column length m with
-// 20*m bytes of shared memory for FP64 terms, 12*m for pattern terms).  Warp 0 sums row i -- its first term itself, then the
-// rest in windows of 32*LLT_SCAN_E terms, each summed as one scan over the warp
-// (trsm_chain.cuh, scan form) and cut short at the first step the scan form does not
-// cover, from where one exact step and the next window go on -- while warps
-// 1..3 compute the terms -a_k,i-1 * b_k of row i-1 (all but its first, whose b_i warp 0
-// is still producing) into the other half of a double buffer.  One barrier per row.
-constexpr int LLT_PC_THREADS = 128;
+// The dot-form solves split over warps (below): the scan form's window parameters.
 constexpr int LLT_SCAN_E = 4;
 constexpr int LLT_SHORT_WINDOW = 64; // a window that ends sooner ...
 constexpr int LLT_SEQ_STEPS = 32;    // ... is followed by this many sequential steps
-
-// t + q[pos] + ... + q[end-1], every addition rounded as p32_add; run by a whole warp,
-// every lane returns the result.  Windows of 32*E addends, E per lane, in the scan form
-// (trsm_chain.cuh): each lane composes its addends' step maps, a warp scan gives every
-// lane its start, every lane walks its addends from the true start, and the window ends
-// at the first step the form does not cover (the running value leaves its binade, the
-// step is risky), which is done exactly before the next window starts.  Where windows
-// keep ending early, short runs of sequential steps (chain_add_run_reg) go in between.
-template <int E, class Q>
-__device__ double warp_chain_scan(double t, Q q, int pos, int end)
-{
-    constexpr unsigned FULL = 0xFFFFFFFFu;
-    const int lane = threadIdx.x & 31;
-    while (pos < end) {
-        SegParams sp;
-        if (!seg_begin(t, sp)) { // zero, or outside the fast window: one exact step
-            t = chain_add_one(t, q[pos]);
-            ++pos;
-            continue;
-        }
-        const int wend = min(end, pos + 32 * E);
-        const int j0 = pos + lane * E;
-        SegFn fe[E];
-        int32_t K[E];
-        bool rk[E];
-        SegFn f = {0, 0};
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const double qv = j0 + e < wend ? q[j0 + e] : 0.0; // 0 is the identity map
-            fe[e] = seg_fn(qv, sp, K[e], rk[e]);
-            f = seg_then(f, fe[e]);
-        }
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            SegFn o;
-            o.c0 = __shfl_up_sync(FULL, f.c0, off);
-            o.c1 = __shfl_up_sync(FULL, f.c1, off);
-            if (lane >= off)
-                f = seg_then(o, f);
-        }
-        SegFn ex;
-        ex.c0 = __shfl_up_sync(FULL, f.c0, 1);
-        ex.c1 = __shfl_up_sync(FULL, f.c1, 1);
-        if (lane == 0)
-            ex = SegFn{0, 0};
-        int32_t M = seg_apply(ex, sp.M0);
-        int jbad = -1;
-        int32_t Mbad = 0;
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const bool live = (jbad < 0) & (j0 + e < wend);
-            const bool ok = seg_valid(M, K[e], rk[e], sp);
-            if (live & !ok) {
-                jbad = j0 + e;
-                Mbad = M;
-            }
-            if (live & ok)
-                M = seg_apply(fe[e], M);
-        }
-        const unsigned bal = __ballot_sync(FULL, jbad >= 0);
-        if (bal == 0) {
-            const int last = (wend - 1 - pos) / E; // the lane holding the window's last addend
-            t = sp.us * (double)__shfl_sync(FULL, M, last);
-            pos = wend;
-        } else {
-            const int src = __ffs(bal) - 1;
-            const int js = __shfl_sync(FULL, jbad, src);
-            const int32_t Ms = __shfl_sync(FULL, Mbad, src);
-            t = chain_add_one(sp.us * (double)Ms, q[js]);
-            // A window cut short means a running value that keeps changing binade (it is
-            // small against its addends): the next LLT_SEQ_STEPS steps go one by one.
-            const bool cut_short = js - pos < LLT_SHORT_WINDOW;
-            pos = js + 1;
-            if (cut_short) {
-                const int cnt = min(LLT_SEQ_STEPS, end - pos);
-                t = chain_add_run_reg(t, q + pos, cnt);
-                pos += cnt;
-            }
-        }
-    }
-    return t;
-}
 
 // Term storage: FP64, or (for long columns) the posit32 patterns of the products.
 template <class T>
@@ -763,83 +674,18 @@ struct LltTerms<uint32_t> {
     __device__ static uint32_t store(uint32_t p) { return p; }
 };
 
-// UPPER: the same solve for an upper triangle, U^-T b (Rtrsm('L', 'U', 'T'),
-// Rtrsm.cpp:160-173), rows in increasing order: row i sums its terms k = 0 .. i-1 in
-// ascending order, so the warp scans the terms k <= i-2 (computed while row i-1 ran) and
-// then adds the last one, -u_{i-1,i} * b_{i-1}, from the value just finished.
-template <class T, bool UPPER = false>
-__global__ void __launch_bounds__(LLT_PC_THREADS) trsm_llt_pc_kernel(const uint32_t *__restrict__ L, size_t ldl,
-                                                                     uint32_t *__restrict__ B, size_t ldb, int m,
-                                                                     bool unit, const int *__restrict__ info)
-{
-    extern __shared__ __align__(16) unsigned char smem_pc[];
-    T *s_q = reinterpret_cast<T *>(smem_pc); // [2][m]: terms
-    uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
-    __shared__ uint32_t s_nar[2];
-    if (info && *info != 0) // a factorization stopped before this solve
-        return;
-    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
-    const int tid = threadIdx.x;
-    for (int k = tid; k < m; k += LLT_PC_THREADS)
-        s_b[k] = bcol[k];
-    if (tid < 2)
-        s_nar[tid] = 0;
-    __syncthreads();
-    uint32_t xprev = 0; // the row finished last, b_{i+1} (lower) or b_{i-1} (upper) (warp 0)
-    for (int step = 0; step < m; ++step) {
-        const int i = UPPER ? step : m - 1 - step;
-        const int cur = step & 1;
-        if (tid < 32) {
-            const uint32_t *li = L + (size_t)i * ldl;
-            const uint32_t bi = s_b[i];
-            uint32_t nar = (bi == P32_NAR) | s_nar[cur];
-            double c = p32_to_double(bi == P32_NAR ? 0u : bi);
-            const typename LltTerms<T>::View q{s_q + (size_t)cur * m};
-            if (!UPPER && i + 1 < m) {
-                c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
-                c = warp_chain_scan<LLT_SCAN_E>(c, q, i + 2, m);
-            }
-            if (UPPER && i >= 1) {
-                c = warp_chain_scan<LLT_SCAN_E>(c, q, 0, i - 1);
-                c = chain_add_one(c, llt_term(li[i - 1], xprev, &nar));
-            }
-            uint32_t t = nar ? P32_NAR : p32_from_double(c);
-            if (!unit)
-                t = pdiv(t, li[i]);
-            xprev = t;
-            __syncwarp();
-            if (tid == 0) {
-                s_b[i] = t;
-                s_nar[cur] = 0;
-            }
-        } else if (step + 1 < m) {
-            // the terms of the next row whose b_k are final: k = i+1 .. m-1 of row i-1
-            // (lower), k = 0 .. i-1 of row i+1 (upper)
-            const int nxt = UPPER ? i + 1 : i - 1;
-            const int kbeg = UPPER ? 0 : i + 1, kend = UPPER ? i : m;
-            const uint32_t *lp = L + (size_t)nxt * ldl;
-            T *qn = s_q + (size_t)(cur ^ 1) * m;
-            uint32_t nar = 0;
-            for (int k = kbeg + (tid - 32); k < kend; k += LLT_PC_THREADS - 32) {
-                const uint32_t p = pmul(0u - s_b[k], lp[k]); // (-b)*a == -(a*b) bit for bit
-                nar |= p == P32_NAR;
-                qn[k] = LltTerms<T>::store(p == P32_NAR ? 0u : p);
-            }
-            if (nar)
-                s_nar[cur ^ 1] = 1;
-        }
-        __syncthreads();
-    }
-    for (int k = tid; k < m; k += LLT_PC_THREADS)
-        bcol[k] = s_b[k];
-}
-
 // ---------------------------------------------------------------------------
-// The same solve with the row's windows spread over a group of warps.
+// The dot-form solve with the row's windows spread over a group of warps.
 // ---------------------------------------------------------------------------
-// One block of 2 * LLT_GROUP_WARPS warps per right-hand side: the first LLT_GROUP_WARPS
-// warps (the consumer group) sum each row in windows of LLT_GROUP_WARPS * 32 * LLT_SCAN_E
-// terms; the others compute the next row's terms meanwhile, as in trsm_llt_pc_kernel.  A
+// Rtrsm('L', 'L', 'T'), Rtrsm.cpp:175-186: for i = m-1 down to 0, t = b_i, t = t - a_ki*b_k
+// for k = i+1 .. m-1 in order, b_i = t / a_ii (UPPER: Rtrsm('L', 'U', 'T'),
+// Rtrsm.cpp:160-173, rows in increasing order, terms k = 0 .. i-1; the warps scan the terms
+// k <= i-2, computed while row i-1 ran, then add the last one from the value just
+// finished).  One block of 2 * LLT_GROUP_WARPS warps per right-hand side: the first
+// LLT_GROUP_WARPS warps (the consumer group) sum each row in windows of
+// LLT_GROUP_WARPS * 32 * LLT_SCAN_E terms in the scan form (trsm_chain.cuh) -- the first term
+// (the b just finished) by one exact step -- while the others compute the next row's terms
+// -a_k * b_k (all whose b_k are final) into the other half of a double buffer.  A
 // window is the warp scan of step maps in every consumer warp, then each warp's composed map
 // goes to shared memory, a named barrier (the consumer group only), each warp composes the
 // maps of the warps before it with its own exclusive prefix and walks its addends, each warp

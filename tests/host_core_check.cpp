@@ -194,7 +194,7 @@ long hc_f64_gemm_chains(const uint32_t *c0, const uint32_t *t, const uint32_t *a
     return fixes;
 }
 
-// One row's chain t + q_0 + ... + q_{len-1} the way lapack.cu's warp_chain_scan runs it,
+// One row's chain t + q_0 + ... + q_{len-1} the way lapack.cu's group_chain_scan runs it,
 // written out sequentially: one warp takes a window of
 // the next 32*E terms, E per lane; each lane's composed map, the exclusive prefix over
 // lanes, every lane's walk from its true start, the first invalid step of the window;
