@@ -316,10 +316,12 @@ PG_HD double chain_add_one(double t, double q)
 // In f64_posit_add the rounding constant is built from the sum's exponent with integer
 // operations on the dependent path.  Within one regime (4 binades) the fraction width is
 // fixed, so C = 2^e * G with G = 1.5 * 2^(52 - fb) the regime's gain, and 2^e is the sum
-// with its sign and fraction bits masked off: one AND and one FP64 multiply.  The regime
-// is taken from the value a block of steps starts at; a step whose sum lands in another
-// regime (or is zero, or is risky as in f64_posit_add) is flagged, and the caller redoes
-// the block with chain_add_one.
+// with its sign and fraction bits masked off: one AND and one FP64 multiply.  The fraction
+// width is that of the value a block of steps starts at; it is the same in regimes k and
+// -k-1 (both have a run of the same length), so the scales [2^-4, 2^4) around 1 form one
+// such range of 8 binades, and the other ranges are single regimes.  A step whose sum
+// lands at another fraction width (or is zero, or is risky as in f64_posit_add) is
+// flagged, and the caller redoes the block with chain_add_one.
 PG_HD double f64_regime_gain(int32_t k)
 {
     const int32_t fb = 28 - ((k ^ (k >> 31)) + 1);
@@ -328,7 +330,14 @@ PG_HD double f64_regime_gain(int32_t k)
 
 PG_HD int32_t f64_regime(double x) { return ((int32_t)((f64_bits(x) >> 52) & 0x7FF) - 1023) >> 2; }
 
-PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint32_t &bad)
+// The regime run length of the scale of FP64 pattern sb (fb = 28 - run).
+PG_HD int32_t f64_bits_run(uint64_t sb)
+{
+    const int32_t k = ((int32_t)((sb >> 52) & 0x7FF) - 1023) >> 2;
+    return (k ^ (k >> 31)) + 1;
+}
+
+PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t run, uint32_t &bad)
 {
     const double s = f64_add(t, q);
     const uint64_t sb = f64_bits(s);
@@ -338,8 +347,7 @@ PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint3
     const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
     const int32_t gap = et > eq ? et - eq : eq - et;
     const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
-    const int32_t ks = ((int32_t)((sb >> 52) & 0x7FF) - 1023) >> 2;
-    bad |= (risky | (ks != kreg)) ? 0x40000000u : 0u;
+    bad |= (risky | (f64_bits_run(sb) != run)) ? 0x40000000u : 0u;
     return r;
 }
 
@@ -351,7 +359,7 @@ PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t kreg, uint3
 // On the dependent path that is one FP64 addition and a few integer operations instead of
 // an AND, an FP64 multiply and two FP64 additions.  sh <= 31: the kept bit and the cleared
 // bits are in the low word.
-PG_HD double f64_posit_add_reg_int(double t, double q, uint32_t sh, int32_t kreg, uint32_t &bad)
+PG_HD double f64_posit_add_reg_int(double t, double q, uint32_t sh, int32_t run, uint32_t &bad)
 {
     const double s = f64_add(t, q);
     const uint64_t sb = f64_bits(s);
@@ -360,8 +368,7 @@ PG_HD double f64_posit_add_reg_int(double t, double q, uint32_t sh, int32_t kreg
     const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
     const int32_t gap = et > eq ? et - eq : eq - et;
     const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
-    const int32_t ks = ((int32_t)((sb >> 52) & 0x7FF) - 1023) >> 2;
-    bad |= (risky | (ks != kreg)) ? 0x40000000u : 0u;
+    bad |= (risky | (f64_bits_run(sb) != run)) ? 0x40000000u : 0u;
     return f64_from_bits(rb);
 }
 
@@ -399,11 +406,11 @@ PG_HD double chain_add_run_reg(double t, Q q, int count)
             const uint32_t sh = 24u + (uint32_t)run;
 #pragma unroll
             for (int j = 0; j < U; ++j)
-                t = f64_posit_add_reg_int(t, v[j], sh, kreg, bad);
+                t = f64_posit_add_reg_int(t, v[j], sh, run, bad);
         } else {
 #pragma unroll
             for (int j = 0; j < U; ++j)
-                t = f64_posit_add_reg(t, v[j], G, kreg, bad);
+                t = f64_posit_add_reg(t, v[j], G, run, bad);
         }
         if (bad & 0x40000000u) { // (from q: a dynamic index into v would put v in local memory)
             t = t0;

@@ -334,14 +334,23 @@ def test_scan_form_of_the_chain_matches_sequential_additions(hc):
     """The scan form of a chain of additions (step maps M -> M + c[M & 1] on the posit grid
     of the running value's binade, composed over a warp's window, cut at the first step the
     form does not cover, short windows followed by sequential runs), and the chain with
-    the rounding constant's regime held fixed over blocks, equal chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
-    cancel to zero, hit ties (halves of the grid spacing), span 80 decades, and carry addends
-    25..30 binades down."""
+    the rounding constant's fraction width held fixed over blocks, equal chain_add_run -- itself pinned to p32_add above -- on chains that stay in one binade, drift across binades,
+    cancel to zero, hit ties (halves of the grid spacing), span 80 decades, carry addends
+    25..30 binades down, and wander across the scales 2^(4j) where the fraction width
+    changes (2^-8, 2^-4, 2^4) or stays (1)."""
     rng = np.random.default_rng(31)
     stats = np.zeros(2, np.int64)
-    for trial in range(1200):
+    for trial in range(1400):
         n = int(rng.integers(0, 1500))
-        kind = trial % 6
+        kind = trial % 7
+        if kind == 6:  # a running value around 2^(4j), steps of about 1/100 of it
+            s4 = 2.0 ** (4 * int(rng.integers(-2, 2)))
+            q = oracle.from_double(rng.uniform(-1, 1, n) * 0.02 * s4)
+            c0 = int(oracle.from_double(np.array([s4 * rng.uniform(0.9, 1.1)]))[0])
+            E = int(rng.choice([1, 4, 16]))
+            assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
+            assert hc.hc_chain_reg_check(c0, np.ascontiguousarray(q), n) == 1, (trial, kind, n, "reg")
+            continue
         if kind == 0:
             q = oracle.from_double(rng.uniform(-1, 1, n) * 0.01)
         elif kind == 1:
