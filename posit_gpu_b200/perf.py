@@ -45,7 +45,7 @@ def fp64_pipe_peak_warp_inst_per_s(sm_mhz):
 # the script that compiles them (flags included); the benchmark recomputes the digest and,
 # when it differs, marks the count stale and reports no roofline fraction from it.
 KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh", "build.py"]
-INST_SOURCE_DIGEST = "fd6a4f522a9b6bbf01d2d31ebff5027198484163ca5c409e99bdad6ddd871c27"
+INST_SOURCE_DIGEST = "0655770ff12d388eae556ca0a5c2fff79a0e8127ce0e6905dc3606f40832bf51"
 
 
 def kernel_source_digest():
