@@ -4,6 +4,7 @@ nvcc for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``), CUDA runtim
 linked statically so the library does not depend on which libcudart the host process
 (e.g. torch) already loaded.  Usage: ``python posit_gpu_b200/build.py [-v]``.
 """
+import glob
 import os
 import subprocess
 import sys
@@ -12,9 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libposit_gpu_b200.so")
 SOURCES = ["gemm.cu", "lapack.cu", "batch.cu", "batch_gemm.cu", "capi.cu", "batch_capi.cu", "noalloc.cu", "serve.cu"]
-HEADERS = ["posit32.cuh", "gemm.cuh", "gemm_tile.cuh", "lapack.cuh", "batch.cuh", "batch_gemm.cuh", "trsm_chain.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-rdc=false"]
 
 
 def _stale(out, deps):
@@ -26,7 +27,7 @@ def _stale(out, deps):
 
 def build(verbose=False, force=False):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
+    deps = srcs + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
         os.path.join(HERE, "..", "include", "posit_gpu.h"), os.path.abspath(__file__)]
     if not force and not _stale(LIB, deps):
         return LIB
@@ -35,8 +36,7 @@ def build(verbose=False, force=False):
     objs = []
     for s in srcs:
         o = os.path.join(objdir, os.path.splitext(os.path.basename(s))[0] + ".o")
-        cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                               "-rdc=false", "-c", s, "-o", o]
+        cmd = [NVCC] + ARCH + CFLAGS + ["-c", s, "-o", o]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         print(" ".join(cmd), flush=True)

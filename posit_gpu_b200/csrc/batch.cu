@@ -103,7 +103,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
                 s_mode = 0;
             } else if ((int32_t)pabs(piv) >= 1) {
                 s_mode = 1;
-                s_recip = pdiv(P32_ONE, piv);
+                s_recip = pdiv_est(P32_ONE, piv);
             } else {
                 s_mode = 2;
             }
@@ -112,8 +112,12 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
         if (piv == 0 && info == 0)
             info = k + 1;
         __syncthreads();
-        if (piv != 0 && p != k) { // interchange whole rows (Rlaswp on both sides)
+        if (p != k) { // interchange whole rows (Rlaswp on both sides)
+            // A zero pivot leaves its own column in place (Rgetrf2.cpp:107-117) while the
+            // recursion's Rlaswp calls still move rows k and p in every other column.
             for (int c = tid; c < n; c += blockDim.x) {
+                if (c == k && piv == 0)
+                    continue;
                 uint32_t *pc = A + (size_t)c * lda;
                 uint32_t t = pc[k];
                 pc[k] = pc[p];
@@ -127,7 +131,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
             if (mode == 1)
                 l = pmul(s_recip, l);
             else if (mode == 2)
-                l = pdiv(l, s_piv);
+                l = pdiv_est(l, s_piv);
             ck[i] = l;
         }
         const bool stage = 2 * n <= STAGE_DOUBLES;
@@ -189,7 +193,7 @@ __device__ void lu_solve_one(const BatchProblem &pr, bool factor, int32_t *s_key
         for (int r = tid; r < nrhs; r += blockDim.x) {
             uint32_t *b = pr.B + (size_t)r * ldb;
             if (b[k] != 0)
-                b[k] = pdiv(b[k], uk[k]);
+                b[k] = pdiv_est(b[k], uk[k]);
         }
         __syncthreads();
         for (int e = tid; e < k * nrhs; e += blockDim.x) {
@@ -218,9 +222,9 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
             uint32_t akk = ck[k];
             s_fail = (int32_t)akk <= 0;
             if (!s_fail) {
-                uint32_t lkk = psqrt(akk);
+                uint32_t lkk = psqrt_est(akk);
                 ck[k] = lkk;
-                s_recip = pdiv(P32_ONE, lkk);
+                s_recip = pdiv_est(P32_ONE, lkk);
             }
         }
         __syncthreads();
@@ -266,7 +270,7 @@ __device__ void chol_solve_one(const BatchProblem &pr, bool factor, uint32_t *s_
         for (int r = tid; r < nrhs; r += blockDim.x) {
             uint32_t *b = pr.B + (size_t)r * ldb;
             if (b[k] != 0)
-                b[k] = pdiv(b[k], lk[k]);
+                b[k] = pdiv_est(b[k], lk[k]);
         }
         __syncthreads();
         const int rows = n - k - 1;

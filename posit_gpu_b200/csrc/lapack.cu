@@ -62,7 +62,8 @@ static size_t panel_ws_bytes(int m) { return 256 + (((size_t)m * 4 + 255) & ~(si
 // column k: iRamax (iRamax.cpp:65-71) over panel-local rows [k, M) -- the first index of
 // the strict maximum of abs() in posit order (signed integer order of the patterns, NaR
 // lowest) -- the interchange of rows k and p over the panel's jb columns
-// (Rgetrf2.cpp:107-117) and the scaling decision (Rgetrf2.cpp:119-131).
+// (Rgetrf2.cpp:107-117; with a zero pivot, over every column but k) and the scaling
+// decision (Rgetrf2.cpp:119-131).
 __global__ void __launch_bounds__(1024) lu_pivot_kernel(uint32_t *__restrict__ P, size_t lda, int M, int jb, int k,
                                                         int row0, int *__restrict__ ipiv, int *__restrict__ info,
                                                         PivotInfo *__restrict__ pinfo,
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(1024) lu_pivot_kernel(uint32_t *__restrict__ P
                 *info = row0 + k + 1;
         } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
             pi.mode = 1;
-            pi.recip = pdiv(P32_ONE, piv);
+            pi.recip = pdiv_est(P32_ONE, piv);
         } else {
             pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
             pi.recip = 0;
@@ -140,8 +141,13 @@ __global__ void __launch_bounds__(1024) lu_pivot_kernel(uint32_t *__restrict__ P
         *pinfo = pi;
     }
     __syncthreads(); // every thread has read the pivot before the rows move
-    if (piv != 0 && p != k) {
+    if (p != k) {
+        // A zero pivot leaves its own column in place (Rgetrf2.cpp:107-117) while the
+        // recursion's Rlaswp calls (Rgetrf2.cpp:141-150, 167-176) still move rows k and p in
+        // every other column of the panel, and Rgetrf's outside it.
         for (int c = tid; c < jb; c += blockDim.x) {
+            if (c == k && piv == 0)
+                continue;
             uint32_t *pc = P + (size_t)c * lda;
             uint32_t t = pc[k];
             pc[k] = pc[p];
@@ -155,7 +161,7 @@ PG_HD uint32_t lu_scaled(uint32_t a, const PivotInfo &pi)
     if (pi.mode == 1)
         return pmul(pi.recip, a); // Rscal: da*dx
     if (pi.mode == 2)
-        return pdiv(a, pi.piv);
+        return pdiv_est(a, pi.piv);
     return a;
 }
 
@@ -190,33 +196,33 @@ __global__ void __launch_bounds__(PANEL_ROWS) lu_update_kernel(uint32_t *__restr
 // LU panel in one thread-block cluster, held in shared memory: the per-column steps of
 // lu_pivot_kernel + lu_update_kernel -- iRamax with first-max tie-break, the interchange
 // across the panel, the scaling decision, the scaled column, the rank-1 update in the FP64
-// step -- in the same per-element order, one launch per panel.  Up to 8 CTAs of 1024
-// threads (8 SMs).  Row i of the panel belongs to thread i mod (CTAs * 1024) for the whole
-// panel and lives in that thread's CTA's shared memory (R rows per thread, jb patterns
-// each), loaded once and written back once.  A thread reads back only what it wrote itself,
-// except at two points per column, each behind a hardware cluster barrier
-// (barrier.cluster, release/acquire at cluster scope; the CTAs of a cluster are
-// co-scheduled, so no barrier waits for a CTA that never runs):
-//   * the pivot candidates: each CTA's best (key, row, value) goes to its shared memory;
-//     every CTA reads all of them through distributed shared memory and decides the pivot
-//     itself (the same bits everywhere);
-//   * the interchange of rows k and p, done by CTA 0 in the owners' shared memory, after
-//     which every CTA reads row k (the -u_kc) from its owner.
-// A final cluster barrier keeps every CTA's shared memory alive until no other CTA reads it.
+// step -- in the same per-element order, one launch per panel.  Up to 8 CTAs of T threads
+// (T a multiple of 32, up to 1024).  The panel's rows are dealt out once, row i to CTA
+// i mod ncta, and there to slot r of thread t with i / ncta = r*T + t (R slots per thread,
+// jb FP64 values each, in shared memory); they never move: an interchange of rows k and p
+// swaps the logical row numbers the two slots hold (each thread keeps its slots' numbers in
+// registers, and every thread knows k and p, so each applies the swap to its own slots),
+// and the write-back stores each slot at the row it holds at the end.  Per column, with the
+// cluster's CTAs co-scheduled (no barrier waits for a CTA that never runs):
+//   * each thread's best (key, logical row, value, slot) over its slots holding rows >= k,
+//     reduced over the warp into the warp's slot in shared memory (double-buffered by
+//     column parity); a cluster barrier (a block barrier with one CTA); every warp reduces
+//     all warps' candidates, read through distributed shared memory -- every thread holds
+//     the pivot, the same bits everywhere;
+//   * threads read -u_kc from the pivot row's slot (in any CTA), one thread per CTA forms
+//     the scaling decision and the reciprocal; a block barrier;
+//   * each thread scales and updates its slots holding rows > k.
+// The pivot row's slot is not written again in the panel (but for a zero pivot below row k,
+// where the two slots trade back their column-k values: that column stays in place,
+// Rgetrf2.cpp:107-117), so reading it after the candidates' barrier races with nothing.  A
+// final cluster barrier keeps every CTA's shared memory alive until no other CTA reads it.
 // ---------------------------------------------------------------------------
-constexpr int PANEL1_THREADS = 1024;
+constexpr int PANEL1_THREADS = 1024;    // most threads per CTA
 constexpr int PANEL1_MAX_JB = 512;
 constexpr int PANEL1_MAX_CTAS = 8;
-constexpr int PANEL1_SMEM_ENTRIES = 24; // R * jb: 8 KB of shared memory (1024 FP64 values) per entry per CTA
-
-// Entry (row i, column c) of the panel in its owner's shared memory, through the cluster.
-__device__ __forceinline__ double *panel_entry(cooperative_groups::cluster_group &cl, double *rows, int jb, int G,
-                                               int i, int c)
-{
-    const int g = i % G, r = i / G;
-    double *base = cl.map_shared_rank(rows, g / PANEL1_THREADS);
-    return base + ((size_t)r * jb + c) * PANEL1_THREADS + (g % PANEL1_THREADS);
-}
+constexpr int PANEL1_SMEM_ENTRIES = 24; // R * jb * T <= 24 * 1024 FP64 values of shared memory per CTA
+constexpr int PANEL1_MAX_R = 4;         // slots per thread (the LU panel keeps their row numbers in registers)
+constexpr int PANEL1_ROWS_PER_CTA = 128; // the rows one CTA takes before another joins
 
 // The barrier of a cluster panel: the cluster's, or the block's when the cluster is one CTA.
 __device__ __forceinline__ void panel_sync(cooperative_groups::cluster_group &cl, int ncta)
@@ -231,6 +237,44 @@ __device__ __forceinline__ void panel_sync(cooperative_groups::cluster_group &cl
 // pabs() on patterns (iRamax.cpp:65-71 compares abs() in posit order).
 __device__ __forceinline__ double pivot_key(double x) { return x != x ? -1.0 : fabs(x); }
 
+// A pivot candidate: the largest key, the first (lowest logical row) among equal keys.
+struct PivotCand {
+    double key, val;
+    int row;  // logical row, -1: none
+    int slot; // (r << 16) | (CTA rank << 10) | thread of the slot holding it
+};
+
+__device__ __forceinline__ void cand_merge(PivotCand &a, const PivotCand &b)
+{
+    if (b.row >= 0 && (a.row < 0 || b.key > a.key || (b.key == a.key && b.row < a.row)))
+        a = b;
+}
+
+__device__ __forceinline__ PivotCand cand_shfl_down(const PivotCand &a, int off)
+{
+    PivotCand b;
+    b.key = __shfl_down_sync(0xFFFFFFFFu, a.key, off);
+    b.val = __shfl_down_sync(0xFFFFFFFFu, a.val, off);
+    b.row = __shfl_down_sync(0xFFFFFFFFu, a.row, off);
+    b.slot = __shfl_down_sync(0xFFFFFFFFu, a.slot, off);
+    return b;
+}
+
+// Warp-wide best candidate, in lane 0 (and, with `all`, broadcast to every lane).
+__device__ __forceinline__ PivotCand cand_warp_reduce(PivotCand a, bool all)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        cand_merge(a, cand_shfl_down(a, off));
+    if (all) {
+        a.key = __shfl_sync(0xFFFFFFFFu, a.key, 0);
+        a.val = __shfl_sync(0xFFFFFFFFu, a.val, 0);
+        a.row = __shfl_sync(0xFFFFFFFFu, a.row, 0);
+        a.slot = __shfl_sync(0xFFFFFFFFu, a.slot, 0);
+    }
+    return a;
+}
+
 __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
                                                                           int M, int jb, int R, int row0,
                                                                           int *__restrict__ ipiv,
@@ -239,88 +283,52 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
-    extern __shared__ __align__(16) double s_rows[]; // [R][jb][1024]: this CTA's rows, FP64
-    __shared__ double s_key[32], s_val[32];
-    __shared__ int s_idx[32];
-    __shared__ double s_ckey, s_cval; // this CTA's pivot candidate (key, value, row), read by
-    __shared__ int s_cidx;            // the whole cluster
-    __shared__ double s_u[PANEL1_MAX_JB]; // -u_kc of the current pivot row
+    extern __shared__ __align__(16) double s_rows[]; // [R][jb][T]: this CTA's slots, FP64
+    __shared__ PivotCand s_wc[2][32];                // each warp's candidate, by column parity
+    __shared__ double s_u[PANEL1_MAX_JB];            // -u_kc of the current pivot row
     __shared__ PivotInfo s_pi;
     __shared__ uint32_t s_tab[F64_CONST_ENTRIES]; // rounding constants (F64ConstTable)
     if (*info < 0) // written only by earlier launches: the same in every CTA
         return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < F64_CONST_ENTRIES; i += PANEL1_THREADS)
+    const int T = (int)blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wpc = T >> 5;
+    for (int i = tid; i < F64_CONST_ENTRIES; i += T)
         s_tab[i] = f64_round_const_top(i);
     const F64ConstTable cof{s_tab}; // read only after the first barrier below
-    const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
-    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
-    for (int r = 0; r < R; ++r) {
-        const int i = g + r * G;
-        if (i < M)
+    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * T + tid]; };
+    int row[PANEL1_MAX_R]; // the logical row each slot holds (-1: none)
+#pragma unroll
+    for (int r = 0; r < PANEL1_MAX_R; ++r) {
+        const int i = (r * T + tid) * ncta + rank;
+        row[r] = (r < R && i < M) ? i : -1;
+        if (row[r] >= 0)
             for (int c = 0; c < jb; ++c)
                 own(r, c) = p32_to_double(P[i + (size_t)c * lda]);
     }
+    const int nslots = ncta * wpc;
     for (int k = 0; k < jb; ++k) {
-        // this thread's rows of [k, M) in increasing order (iRamax.cpp:65-71), first max wins
-        double best = -2.0, bval = 0.0;
-        int bidx = -1;
-        for (int r = 0; r < R; ++r) {
-            const int i = g + r * G;
-            if (i >= k && i < M) {
-                const double v = own(r, k), key = pivot_key(v);
-                if (bidx < 0 || key > best) {
-                    best = key;
-                    bidx = i;
-                    bval = v;
-                }
-            }
-        }
+        PivotCand cand = {-2.0, 0.0, -1, 0};
 #pragma unroll
-        for (int round = 0; round < 2; ++round) {
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double k2 = __shfl_down_sync(0xFFFFFFFFu, best, off);
-                const double v2 = __shfl_down_sync(0xFFFFFFFFu, bval, off);
-                const int i2 = __shfl_down_sync(0xFFFFFFFFu, bidx, off);
-                if (i2 >= 0 && (bidx < 0 || k2 > best || (k2 == best && i2 < bidx))) {
-                    best = k2;
-                    bidx = i2;
-                    bval = v2;
-                }
+        for (int r = 0; r < PANEL1_MAX_R; ++r)
+            if (row[r] >= k) {
+                const double v = own(r, k);
+                cand_merge(cand, PivotCand{pivot_key(v), v, row[r], (r << 16) | (rank << 10) | tid});
             }
-            if (round == 0) {
-                if (lane == 0) {
-                    s_key[warp] = best;
-                    s_idx[warp] = bidx;
-                    s_val[warp] = bval;
-                }
-                __syncthreads();
-                const bool slot = lane < (int)(blockDim.x >> 5); // one slot per warp of the block
-                best = slot ? s_key[lane] : -2.0;
-                bidx = slot ? s_idx[lane] : -1;
-                bval = slot ? s_val[lane] : 0.0;
-            }
-        }
-        if (tid == 0) {
-            s_ckey = best;
-            s_cidx = bidx;
-            s_cval = bval;
-        }
-        panel_sync(cluster, ncta); // candidates visible
-        if (tid == 0) {
-            int p = -1;
-            double pk = -2.0, pv = 0.0;
-            for (int r = 0; r < ncta; ++r) {
-                const double k2 = *cluster.map_shared_rank(&s_ckey, r);
-                const int i2 = *cluster.map_shared_rank(&s_cidx, r);
-                if (i2 >= 0 && (p < 0 || k2 > pk || (k2 == pk && i2 < p))) {
-                    pk = k2;
-                    p = i2;
-                    pv = *cluster.map_shared_rank(&s_cval, r); // the row itself may move meanwhile
-                }
-            }
-            const uint32_t piv = p32_from_double_exact(pv);
+        cand = cand_warp_reduce(cand, false);
+        if (lane == 0)
+            s_wc[k & 1][warp] = cand;
+        panel_sync(cluster, ncta); // the warps' candidates, cluster-wide
+        cand = PivotCand{-2.0, 0.0, -1, 0};
+        for (int s = lane; s < nslots; s += 32)
+            cand_merge(cand, *cluster.map_shared_rank(&s_wc[k & 1][s % wpc], s / wpc));
+        cand = cand_warp_reduce(cand, true);
+        const int p = cand.row;
+        const uint32_t piv = p32_from_double_exact(cand.val);
+        // u from the pivot row's slot (after the interchange it is row k)
+        const int sr = cand.slot >> 16, sq = (cand.slot >> 10) & 63, st = cand.slot & 1023;
+        double *src = cluster.map_shared_rank(s_rows, sq) + (size_t)sr * jb * T + st;
+        for (int c = k + 1 + tid; c < jb; c += T)
+            s_u[c] = -src[(size_t)c * T];
+        if (tid == T - 1) {
             PivotInfo pi;
             pi.row = p;
             pi.piv = piv;
@@ -331,7 +339,7 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
                     *info = row0 + k + 1;
             } else if ((int32_t)pabs(piv) >= (int32_t)1u) { // |pivot| >= sfmin = FLT_MIN -> minpos
                 pi.mode = 1;
-                pi.recip = pdiv(P32_ONE, piv);
+                pi.recip = pdiv_est(P32_ONE, piv);
             } else {
                 pi.mode = 2; // NaR pivot: element-wise division (Rgetrf2.cpp:124-126)
                 pi.recip = 0;
@@ -340,44 +348,45 @@ __global__ void __launch_bounds__(PANEL1_THREADS) lu_panel_cluster_kernel(uint32
                 ipiv[row0 + k] = row0 + p + 1; // 1-based, global
             s_pi = pi;
         }
-        __syncthreads();
-        const PivotInfo pi = s_pi;
-        if (rank == 0 && pi.piv != 0 && pi.row != k) { // Rgetrf2.cpp:107-117
-            for (int c = tid; c < jb; c += PANEL1_THREADS) {
-                double *ek = panel_entry(cluster, s_rows, jb, G, k, c);
-                double *ep = panel_entry(cluster, s_rows, jb, G, pi.row, c);
-                const double t = *ek;
-                *ek = *ep;
-                *ep = t;
+        if (p != k) {
+            if (piv == 0) {
+                // A zero pivot leaves its own column in place (Rgetrf2.cpp:107-117) while the
+                // recursion's Rlaswp calls move rows k and p in every other column: the two
+                // slots trade their column-k values back.  Only row k's holder touches them
+                // (the pivot's slot is read above at columns > k only).
+#pragma unroll
+                for (int r = 0; r < PANEL1_MAX_R; ++r)
+                    if (row[r] == k) {
+                        src[(size_t)k * T] = own(r, k);
+                        own(r, k) = cand.val;
+                    }
             }
+#pragma unroll
+            for (int r = 0; r < PANEL1_MAX_R; ++r)
+                row[r] = row[r] == k ? p : (row[r] == p ? k : row[r]);
         }
-        panel_sync(cluster, ncta); // the interchange is visible
-        for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_u[c] = -*panel_entry(cluster, s_rows, jb, G, k, c);
-        __syncthreads();
+        __syncthreads(); // u and the scaling decision
+        const PivotInfo pi = s_pi;
         const double drecip = p32_to_double(pi.recip);
-        for (int r = 0; r < R; ++r) {
-            const int i = g + r * G;
-            if (i > k && i < M) {
-                double *row = &own(r, 0);
+#pragma unroll
+        for (int r = 0; r < PANEL1_MAX_R; ++r) {
+            if (row[r] > k) {
+                double *rw = &own(r, 0);
                 // Rscal (x*recip, the FP64 product step) or the element-wise division
-                const double dl = pi.mode == 1 ? f64_posit_mul_checked(row[(size_t)k * PANEL1_THREADS], drecip, cof)
-                                               : p32_to_double(lu_scaled(
-                                                     p32_from_double_exact(row[(size_t)k * PANEL1_THREADS]), pi));
-                row[(size_t)k * PANEL1_THREADS] = dl;
+                const double dl = pi.mode == 1 ? f64_posit_mul_checked(rw[(size_t)k * T], drecip, cof)
+                                               : p32_to_double(lu_scaled(p32_from_double_exact(rw[(size_t)k * T]), pi));
+                rw[(size_t)k * T] = dl;
                 for (int c = k + 1; c < jb; ++c) // a_ic + (-u_kc)*l_i in the FP64 step
-                    row[(size_t)c * PANEL1_THREADS] =
-                        f64_posit_mac_checked(row[(size_t)c * PANEL1_THREADS], s_u[c], dl, cof);
+                    rw[(size_t)c * T] = f64_posit_mac_checked(rw[(size_t)c * T], s_u[c], dl, cof);
             }
         }
     }
     panel_sync(cluster, ncta); // no CTA leaves while another may still read its shared memory
-    for (int r = 0; r < R; ++r) {
-        const int i = g + r * G;
-        if (i < M)
+#pragma unroll
+    for (int r = 0; r < PANEL1_MAX_R; ++r)
+        if (row[r] >= 0)
             for (int c = 0; c < jb; ++c)
-                P[i + (size_t)c * lda] = p32_from_double_exact(own(r, c));
-    }
+                P[row[r] + (size_t)c * lda] = p32_from_double_exact(own(r, c));
 }
 
 // After a panel of columns [j, j+jb) (jb <= ROWS_JB_MAX): the panel's row interchanges
@@ -538,7 +547,7 @@ __global__ void trsm_lln_kernel(const uint32_t *__restrict__ L, size_t ldl, uint
         double bk = x.get(k);
         if (bk != 0.0) {
             if (!unit) {
-                bk = p32_to_double(pdiv(p32_from_double(bk), L[k + (size_t)k * ldl]));
+                bk = p32_to_double(pdiv_est(p32_from_double(bk), L[k + (size_t)k * ldl]));
                 __syncthreads();
                 if (threadIdx.x == 0)
                     x.set(k, bk);
@@ -573,7 +582,7 @@ __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint
         double bk = x.get(k);
         if (bk != 0.0) {
             if (!unit) {
-                bk = p32_to_double(pdiv(p32_from_double(bk), U[k + (size_t)k * ldu]));
+                bk = p32_to_double(pdiv_est(p32_from_double(bk), U[k + (size_t)k * ldu]));
                 __syncthreads();
                 if (threadIdx.x == 0)
                     x.set(k, bk);
@@ -590,11 +599,115 @@ __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint
             bcol[i] = p32_from_double(s_x[i]);
 }
 
-// Forward / backward solve launches: staged when the column fits in shared memory.
+// The same two solves with the column staged in shared memory and each thread's rows of
+// the triangle's next column (and the next diagonal) loaded into registers while the
+// current step runs, so no step waits for memory: rows tid + j*T (j < J) belong to thread
+// tid.  The division's result b_k is stored at the start of the next step (every thread has
+// read b_k before the step's barrier), so a step has one barrier.
+template <bool UPPER, int J>
+__global__ void __launch_bounds__(1024) trsm_col_kernel(const uint32_t *__restrict__ A, size_t lda,
+                                                        uint32_t *__restrict__ B, size_t ldb, int m, bool unit,
+                                                        const int *__restrict__ info)
+{
+    extern __shared__ double s_x[];
+    if (info && *info < 0)
+        return;
+    uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
+    const int T = (int)blockDim.x, tid = threadIdx.x;
+    for (int i = tid; i < m; i += T)
+        s_x[i] = p32_to_double(bcol[i]);
+    auto step_col = [&](int st) { return UPPER ? m - 1 - st : st; };
+    uint32_t lc[J], ln[J];
+    uint32_t dc = 0, dn = 0;
+    {
+        const int k = step_col(0);
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int i = tid + j * T;
+            lc[j] = i < m ? A[i + (size_t)k * lda] : 0u;
+        }
+        if (!unit)
+            dc = A[k + (size_t)k * lda];
+    }
+    __syncthreads();
+    int pend_k = -1; // thread 0: b_k divided in the last step, stored at the start of this one
+    double pend_v = 0.0;
+    for (int st = 0; st < m; ++st) {
+        const int k = step_col(st);
+        if (st + 1 < m) {
+            const int kn = step_col(st + 1);
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int i = tid + j * T;
+                ln[j] = i < m ? A[i + (size_t)kn * lda] : 0u;
+            }
+            if (!unit)
+                dn = A[kn + (size_t)kn * lda];
+        }
+        if (pend_k >= 0) {
+            s_x[pend_k] = pend_v;
+            pend_k = -1;
+        }
+        double bk = s_x[k];
+        if (bk != 0.0) { // zero multipliers skipped (Rtrsm.cpp:125-126, 143-144)
+            if (!unit) {
+                bk = p32_to_double(pdiv_est(p32_from_double_exact(bk), dc));
+                if (tid == 0) {
+                    pend_k = k;
+                    pend_v = bk;
+                }
+            }
+            const double nb = -bk;
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int i = tid + j * T;
+                if (UPPER ? i < k : (i > k && i < m))
+                    s_x[i] = trsm_update(s_x[i], nb, p32_to_double(lc[j]));
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            lc[j] = ln[j];
+        dc = dn;
+    }
+    if (pend_k >= 0)
+        s_x[pend_k] = pend_v;
+    __syncthreads();
+    for (int i = tid; i < m; i += T)
+        bcol[i] = p32_from_double_exact(s_x[i]);
+}
+
+template <bool UPPER>
+static cudaError_t launch_col(int J, int nrhs, int threads, const uint32_t *A, size_t lda, uint32_t *B, size_t ldb,
+                              int m, bool unit, const int *info, cudaStream_t st)
+{
+    const size_t bytes = (size_t)m * sizeof(double);
+    const void *fn = J <= 1 ? (const void *)trsm_col_kernel<UPPER, 1>
+                   : J <= 2 ? (const void *)trsm_col_kernel<UPPER, 2>
+                   : J <= 4 ? (const void *)trsm_col_kernel<UPPER, 4>
+                   : J <= 8 ? (const void *)trsm_col_kernel<UPPER, 8>
+                            : (const void *)trsm_col_kernel<UPPER, 16>;
+    if (bytes > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess)
+            return e;
+    }
+    void *args[] = {(void *)&A, (void *)&lda, (void *)&B, (void *)&ldb, (void *)&m, (void *)&unit, (void *)&info};
+    return cudaLaunchKernel(fn, dim3((unsigned)nrhs), dim3((unsigned)threads), args, bytes, st);
+}
+
+// Forward / backward solve launches: staged when the column fits in shared memory (with
+// the prefetching kernel up to 16 rows per thread).
 static cudaError_t launch_lln(int nrhs, int threads, const uint32_t *L, size_t ldl, uint32_t *B, size_t ldb,
                               int m, bool unit, const int *info, cudaStream_t st)
 {
     const size_t bytes = (size_t)m * sizeof(double);
+    const int J = (m + threads - 1) / threads;
+    if (bytes <= 227 * 1024 && J <= 16) {
+        const cudaError_t e = launch_col<false>(J, nrhs, threads, L, ldl, B, ldb, m, unit, info, st);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     if (bytes <= 227 * 1024) {
         if (bytes > 48 * 1024) {
             const cudaError_t e = cudaFuncSetAttribute(trsm_lln_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -613,6 +726,11 @@ static cudaError_t launch_lun(int nrhs, int threads, const uint32_t *U, size_t l
                               int m, bool unit, const int *info, cudaStream_t st)
 {
     const size_t bytes = (size_t)m * sizeof(double);
+    const int J = (m + threads - 1) / threads;
+    if (bytes <= 227 * 1024 && J <= 16) {
+        const cudaError_t e = launch_col<true>(J, nrhs, threads, U, ldu, B, ldb, m, unit, info, st);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     if (bytes <= 227 * 1024) {
         if (bytes > 48 * 1024) {
             const cudaError_t e = cudaFuncSetAttribute(trsm_lun_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -696,21 +814,25 @@ struct LltTerms<uint32_t> {
 constexpr int LLT_GROUP_WARPS = 4;
 constexpr int LLT_GROUP_THREADS = 2 * LLT_GROUP_WARPS * 32;
 
-struct GroupScan {
-    SegFn wt[LLT_GROUP_WARPS]; // each consumer warp's composed map
-    int jbad[LLT_GROUP_WARPS]; // each warp's first uncovered step (-1: none)
-    int32_t Mbad[LLT_GROUP_WARPS];
-    int32_t Mend; // M after the window's last addend
+// One window's exchange between the consumer warps; two of them, used by turns, so that a
+// window's results may be read while the next window's are written.
+struct __align__(16) GroupScan {
+    SegFn wt[LLT_GROUP_WARPS];     // each consumer warp's composed map
+    int jbad[LLT_GROUP_WARPS];     // each warp's first uncovered step (-1: none)
+    int32_t Mbad[LLT_GROUP_WARPS]; // M before that step
+    int32_t Mend;                  // M after the window's last addend
 };
+static_assert(LLT_GROUP_WARPS == 4, "the window's results are read as int4 vectors");
 
 __device__ __forceinline__ void group_bar() { asm volatile("bar.sync 1, %0;" ::"r"(LLT_GROUP_WARPS * 32) : "memory"); }
 
 template <int E, class Q>
-__device__ double group_chain_scan(double t, Q q, int pos, int end, GroupScan *gs)
+__device__ double group_chain_scan(double t, Q q, int pos, int end, GroupScan *gsb, int &turn)
 {
     constexpr unsigned FULL = 0xFFFFFFFFu;
     const int ct = threadIdx.x, lane = ct & 31, w = ct >> 5;
     while (pos < end) {
+        GroupScan *gs = gsb + turn;
         SegParams sp;
         if (!seg_begin(t, sp)) { // zero, or outside the fast window: one exact step
             t = chain_add_one(t, q[pos]);
@@ -745,9 +867,15 @@ __device__ double group_chain_scan(double t, Q q, int pos, int end, GroupScan *g
         if (lane == 31)
             gs->wt[w] = f;
         group_bar();
+        const int4 wt01 = *reinterpret_cast<const int4 *>(&gs->wt[0]);
+        const int4 wt23 = *reinterpret_cast<const int4 *>(&gs->wt[2]);
         SegFn pre = {0, 0};
-        for (int v = 0; v < w; ++v)
-            pre = seg_then(pre, gs->wt[v]);
+        if (w > 0)
+            pre = SegFn{wt01.x, wt01.y};
+        if (w > 1)
+            pre = seg_then(pre, SegFn{wt01.z, wt01.w});
+        if (w > 2)
+            pre = seg_then(pre, SegFn{wt23.x, wt23.y});
         int32_t M = seg_apply(seg_then(pre, ex), sp.M0);
         int jbad = -1;
         int32_t Mbad = 0;
@@ -773,16 +901,19 @@ __device__ double group_chain_scan(double t, Q q, int pos, int end, GroupScan *g
         if (ct == (wend - 1 - pos) / E) // the thread holding the window's last addend
             gs->Mend = M;
         group_bar();
-        int js = -1;
-        int32_t Ms = 0;
-        for (int v = 0; v < LLT_GROUP_WARPS; ++v)
-            if (gs->jbad[v] >= 0) {
-                js = gs->jbad[v];
-                Ms = gs->Mbad[v];
-                break;
-            }
+        // the first warp's first uncovered step (warps hold increasing positions)
+        const int4 jb4 = *reinterpret_cast<const int4 *>(gs->jbad);
+        const int4 mb4 = *reinterpret_cast<const int4 *>(gs->Mbad);
         const int32_t Me = gs->Mend;
-        group_bar(); // every consumer has read the window's results before the next one
+        int js = jb4.w;
+        int32_t Ms = mb4.w;
+        if (jb4.z >= 0) { js = jb4.z; Ms = mb4.z; }
+        if (jb4.y >= 0) { js = jb4.y; Ms = mb4.y; }
+        if (jb4.x >= 0) { js = jb4.x; Ms = mb4.x; }
+        // The next window writes the other exchange; this one is written again only after
+        // the next window's first group barrier, which every consumer reaches after the
+        // reads above.
+        turn ^= 1;
         if (js < 0) {
             t = sp.us * (double)Me;
             pos = wend;
@@ -810,7 +941,7 @@ __global__ void __launch_bounds__(LLT_GROUP_THREADS) trsm_ltx_group_kernel(const
     T *s_q = reinterpret_cast<T *>(smem_pc); // [2][m]: terms
     uint32_t *s_b = reinterpret_cast<uint32_t *>(s_q + 2 * (size_t)m);
     __shared__ uint32_t s_nar[2];
-    __shared__ GroupScan s_gs;
+    __shared__ GroupScan s_gs[2];
     if (info && *info != 0) // a factorization stopped before this solve
         return;
     uint32_t *bcol = B + (size_t)blockIdx.x * ldb;
@@ -822,6 +953,7 @@ __global__ void __launch_bounds__(LLT_GROUP_THREADS) trsm_ltx_group_kernel(const
         s_nar[tid] = 0;
     __syncthreads();
     uint32_t xprev = 0; // the row finished last, b_{i+1} (lower) or b_{i-1} (upper) (consumers)
+    int turn = 0;       // which of s_gs the next window uses (consumers)
     for (int step = 0; step < m; ++step) {
         const int i = UPPER ? step : m - 1 - step;
         const int cur = step & 1;
@@ -833,15 +965,15 @@ __global__ void __launch_bounds__(LLT_GROUP_THREADS) trsm_ltx_group_kernel(const
             const typename LltTerms<T>::View q{s_q + (size_t)cur * m};
             if (!UPPER && i + 1 < m) {
                 c = chain_add_one(c, llt_term(li[i + 1], xprev, &nar));
-                c = group_chain_scan<LLT_SCAN_E>(c, q, i + 2, m, &s_gs);
+                c = group_chain_scan<LLT_SCAN_E>(c, q, i + 2, m, s_gs, turn);
             }
             if (UPPER && i >= 1) {
-                c = group_chain_scan<LLT_SCAN_E>(c, q, 0, i - 1, &s_gs);
+                c = group_chain_scan<LLT_SCAN_E>(c, q, 0, i - 1, s_gs, turn);
                 c = chain_add_one(c, llt_term(li[i - 1], xprev, &nar));
             }
             uint32_t t = nar ? P32_NAR : p32_from_double(c);
             if (!unit)
-                t = pdiv(t, li[i]);
+                t = pdiv_est(t, li[i]);
             xprev = t;
             group_bar(); // every consumer has read s_nar[cur]
             if (tid == 0) {
@@ -911,8 +1043,8 @@ __global__ void chol_diag_kernel(uint32_t *__restrict__ P, size_t lda, int M, in
         if (s_stop) {
             *info = row0 + k + 1;
         } else {
-            uint32_t lkk = psqrt(akk);
-            s_recip = pdiv(P32_ONE, lkk);
+            uint32_t lkk = psqrt_est(akk);
+            s_recip = pdiv_est(P32_ONE, lkk);
             pk[k] = lkk;
             sync->recip = s_recip;
         }
@@ -953,15 +1085,15 @@ __global__ void __launch_bounds__(PANEL_ROWS) chol_update_kernel(uint32_t *__res
     }
 }
 
-// Lower Cholesky panel in one thread-block cluster, held in shared memory with the same
-// row ownership as lu_panel_cluster_kernel, the counterpart of chol_diag_kernel +
-// chol_update_kernel.  Per column: a cluster barrier; every CTA reads the final a_kk from
-// its owner and takes its square root and reciprocal (Rpotrf2.cpp:90-97; the same bits
-// everywhere); each thread scales its rows below the diagonal (Rtrsm.cpp:265-268); a
-// cluster barrier; CTA 0 stores l_kk with its owner (no CTA reads a_kk after that
-// barrier); every CTA reads the panel rows' -l_ck; each thread updates its rows.  A
-// failed diagonal (info) ends the loop in every CTA at the same column; the rows are
-// written back either way.
+// Lower Cholesky panel in one thread-block cluster, held in shared memory (rows dealt out
+// as in lu_panel_cluster_kernel; here they never change places), the counterpart of
+// chol_diag_kernel + chol_update_kernel.  The thread holding row k forms l_kk and 1/l_kk
+// (Rpotrf2.cpp:90-97) right after its own update of column k-1 and writes the decision and
+// 1/l_kk into every CTA.  Per column: a cluster barrier (A); every thread scales its rows
+// below the diagonal (Rtrsm.cpp:265-268), the holders of the diagonal block's rows also
+// writing their -l_ck into every CTA; a cluster barrier (B); each thread updates its rows.
+// With one CTA the barriers are the block's.  A failed diagonal (info) ends the loop in
+// every CTA at the same column; the rows are written back either way.
 __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint32_t *__restrict__ P, size_t lda,
                                                                             int M, int jb, int R, int row0,
                                                                             int *__restrict__ info)
@@ -969,68 +1101,80 @@ __global__ void __launch_bounds__(PANEL1_THREADS) chol_panel_cluster_kernel(uint
     namespace cgs = cooperative_groups;
     cgs::cluster_group cluster = cgs::this_cluster();
     const int rank = (int)cluster.block_rank(), ncta = (int)cluster.num_blocks();
-    extern __shared__ __align__(16) double s_rows[]; // [R][jb][1024]: this CTA's rows, FP64
+    extern __shared__ __align__(16) double s_rows[]; // [R][jb][T]: this CTA's rows, FP64
     __shared__ double s_l[PANEL1_MAX_JB];           // -l_ck of the current column
-    __shared__ uint32_t s_recip, s_lkk;
-    __shared__ int s_stop;
-    __shared__ uint32_t s_tab[F64_CONST_ENTRIES]; // rounding constants (F64ConstTable)
+    __shared__ uint32_t s_recip;                    // 1/l_kk
+    __shared__ int s_stop;                          // a_kk <= 0 or NaR
+    __shared__ uint32_t s_tab[F64_CONST_ENTRIES];   // rounding constants (F64ConstTable)
     if (*info != 0) // written only by earlier launches: the same in every CTA
         return;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < F64_CONST_ENTRIES; i += PANEL1_THREADS)
+    const int T = (int)blockDim.x, tid = threadIdx.x;
+    for (int i = tid; i < F64_CONST_ENTRIES; i += T)
         s_tab[i] = f64_round_const_top(i);
     const F64ConstTable cof{s_tab}; // read only after the first barrier below
-    const int G = ncta * PANEL1_THREADS, g = rank * PANEL1_THREADS + tid;
-    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * PANEL1_THREADS + tid]; };
+    auto own = [&](int r, int c) -> double & { return s_rows[((size_t)r * jb + c) * T + tid]; };
+    auto row_of = [&](int r) { return (r * T + tid) * ncta + rank; };
     for (int r = 0; r < R; ++r) {
-        const int i = g + r * G;
+        const int i = row_of(r);
         if (i < M)
             for (int c = 0; c < jb; ++c)
                 own(r, c) = p32_to_double(P[i + (size_t)c * lda]);
     }
-    for (int k = 0; k < jb; ++k) {
-        panel_sync(cluster, ncta); // every update of column k is done
-        if (tid == 0) {
-            const uint32_t akk = p32_from_double_exact(*panel_entry(cluster, s_rows, jb, G, k, k));
-            s_stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
-            if (s_stop) {
-                if (rank == 0)
-                    *info = row0 + k + 1;
-            } else {
-                s_lkk = psqrt(akk);
-                s_recip = pdiv(P32_ONE, s_lkk);
-            }
+    // From the holder of row k: l_kk in place, the decision and 1/l_kk into every CTA.
+    auto diag = [&](int r, int k) {
+        const uint32_t akk = p32_from_double_exact(own(r, k));
+        const int stop = (int32_t)akk <= 0; // NaR included (Rpotrf2.cpp:90-93)
+        uint32_t recip = 0;
+        if (!stop) {
+            const uint32_t lkk = psqrt_est(akk);
+            own(r, k) = p32_to_double(lkk);
+            recip = pdiv_est(P32_ONE, lkk);
         }
-        __syncthreads();
-        if (s_stop) // decided from the same a_kk in every CTA
+        for (int q = 0; q < ncta; ++q) {
+            *cluster.map_shared_rank(&s_stop, q) = stop;
+            *cluster.map_shared_rank(&s_recip, q) = recip;
+        }
+    };
+    panel_sync(cluster, ncta); // every CTA has started: distributed shared memory may be written
+    for (int r = 0; r < R; ++r)
+        if (row_of(r) == 0)
+            diag(r, 0);
+    for (int k = 0; k < jb; ++k) {
+        panel_sync(cluster, ncta); // A: the decision and 1/l_kk; every read of the last column's -l_ck done
+        if (s_stop) { // the same in every CTA
+            // written only here, after every CTA has passed its entry check of *info
+            if (rank == 0 && tid == 0)
+                *info = row0 + k + 1;
             break;
+        }
         const double drecip = p32_to_double(s_recip);
         for (int r = 0; r < R; ++r) {
-            const int i = g + r * G;
-            if (i > k && i < M) // (1/l_kk)*a_ik, the FP64 product step
-                own(r, k) = f64_posit_mul_checked(own(r, k), drecip, cof);
+            const int i = row_of(r);
+            if (i > k && i < M) { // (1/l_kk)*a_ik, the FP64 product step
+                const double l = f64_posit_mul_checked(own(r, k), drecip, cof);
+                own(r, k) = l;
+                if (i < jb)
+                    for (int q = 0; q < ncta; ++q)
+                        *cluster.map_shared_rank(&s_l[i], q) = -l;
+            }
         }
-        panel_sync(cluster, ncta); // the scaled column is visible, and every CTA has read a_kk
-        if (rank == 0 && tid == 0)
-            *panel_entry(cluster, s_rows, jb, G, k, k) = p32_to_double(s_lkk);
-        for (int c = k + 1 + tid; c < jb; c += PANEL1_THREADS)
-            s_l[c] = -*panel_entry(cluster, s_rows, jb, G, c, k);
-        __syncthreads();
+        panel_sync(cluster, ncta); // B: the column's -l_ck in every CTA
         for (int r = 0; r < R; ++r) {
-            const int i = g + r * G;
+            const int i = row_of(r);
             if (i > k && i < M) {
-                double *row = &own(r, 0);
-                const double dl = row[(size_t)k * PANEL1_THREADS];
+                double *rw = &own(r, 0);
+                const double dl = rw[(size_t)k * T];
                 const int cend = min(jb - 1, i);
                 for (int c = k + 1; c <= cend; ++c) // a_ic + (-l_ck)*l_i in the FP64 step
-                    row[(size_t)c * PANEL1_THREADS] =
-                        f64_posit_mac_checked(row[(size_t)c * PANEL1_THREADS], s_l[c], dl, cof);
+                    rw[(size_t)c * T] = f64_posit_mac_checked(rw[(size_t)c * T], s_l[c], dl, cof);
+                if (i == k + 1 && i < jb) // the next diagonal, from its holder's own update
+                    diag(r, k + 1);
             }
         }
     }
-    panel_sync(cluster, ncta); // l_kk stored; no CTA leaves while another may still read its shared memory
+    panel_sync(cluster, ncta); // no CTA leaves while another may still write its shared memory
     for (int r = 0; r < R; ++r) {
-        const int i = g + r * G;
+        const int i = row_of(r);
         if (i < M)
             for (int c = 0; c < jb; ++c)
                 P[i + (size_t)c * lda] = p32_from_double_exact(own(r, c));
@@ -1083,7 +1227,7 @@ __global__ void __launch_bounds__(POTRF2_CTA_THREADS) potrf2_upper_cta_kernel(ui
                     *info = row0 + off + 1;
                     s_stop = 1;
                 } else {
-                    *d = psqrt(a);
+                    *d = psqrt_est(a);
                 }
                 s_sp = sp - 1;
             }
@@ -1108,7 +1252,7 @@ __global__ void __launch_bounds__(POTRF2_CTA_THREADS) potrf2_upper_cta_kernel(ui
                         double t = p32_to_double(b[i]);
                         for (int k = 0; k < i; ++k)
                             t = f64_posit_mac_checked(t, -p32_to_double(b[k]), p32_to_double(ui[k]));
-                        b[i] = pdiv(p32_from_double(t), ui[i]);
+                        b[i] = pdiv_est(p32_from_double(t), ui[i]);
                     }
                 }
                 __syncthreads();
@@ -1179,33 +1323,35 @@ size_t rgetrf_workspace_bytes(int m, int n, int nb)
 }
 
 // The panel form: the cluster panel held in shared memory when its rows fit (ncta CTAs,
-// one per 1024 rows up to 8, R rows per thread, R * jb <= PANEL1_SMEM_ENTRIES), else the
-// two-launch form (ncta = 0).
+// one per PANEL1_ROWS_PER_CTA rows up to 8, T threads each -- the CTA's rows rounded up to
+// whole warps, at most 1024 -- R slots per thread, R * jb * T FP64 values of shared memory
+// at most 24 * 1024), else the two-launch form (ncta = 0).
 struct PanelForm {
-    int ncta, R;
+    int ncta, R, T; // CTAs (0: the panel does not fit), slots per thread, threads per CTA
 };
 static PanelForm panel_form(int M, int jb)
 {
     if (jb > PANEL1_MAX_JB)
-        return {0, 0};
-    const int ncta = std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_THREADS - 1) / PANEL1_THREADS));
-    const int G = ncta * PANEL1_THREADS, R = (M + G - 1) / G;
-    if (R * jb > PANEL1_SMEM_ENTRIES)
-        return {0, 0};
-    return {ncta, R};
+        return {0, 0, 0};
+    const int ncta = std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_ROWS_PER_CTA - 1) / PANEL1_ROWS_PER_CTA));
+    const int rpc = (M + ncta - 1) / ncta; // rows per CTA
+    const int T = std::min(PANEL1_THREADS, (rpc + 31) / 32 * 32), R = (rpc + T - 1) / T;
+    if ((size_t)R * jb * T > (size_t)PANEL1_SMEM_ENTRIES * PANEL1_THREADS || R > PANEL1_MAX_R)
+        return {0, 0, 0};
+    return {ncta, R, T};
 }
 
 template <class... Args>
 static cudaError_t launch_panel_cluster(void (*kernel)(Args...), PanelForm f, int jb, cudaStream_t st, Args... args)
 {
-    const size_t smem = (size_t)f.R * jb * PANEL1_THREADS * sizeof(double);
+    const size_t smem = (size_t)f.R * jb * f.T * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          PANEL1_SMEM_ENTRIES * PANEL1_THREADS * (int)sizeof(double));
     if (e != cudaSuccess)
         return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)f.ncta);
-    cfg.blockDim = dim3(PANEL1_THREADS);
+    cfg.blockDim = dim3((unsigned)f.T);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];

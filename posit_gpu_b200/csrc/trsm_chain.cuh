@@ -21,6 +21,7 @@
 // block's operands are loaded (clamped to stay in bounds) while the current one runs.
 #pragma once
 #include "posit32.cuh"
+#include "posit32_div.cuh"
 #include <math.h>
 
 namespace pg {
@@ -96,7 +97,7 @@ PG_HD void llt_chain(const uint32_t *__restrict__ L, size_t ldl, uint32_t *b, in
         }
         uint32_t t = nar ? P32_NAR : encode(c);
         if (!unit)
-            t = pdiv(t, li[i]);
+            t = pdiv_est(t, li[i]);
         b[i] = t;
     }
 }
@@ -311,23 +312,22 @@ PG_HD double chain_add_one(double t, double q)
 
 
 // ---------------------------------------------------------------------------
-// The chain step with the regime held fixed.
+// The chain step with the fraction width held fixed.
 // ---------------------------------------------------------------------------
 // In f64_posit_add the rounding constant is built from the sum's exponent with integer
-// operations on the dependent path.  Within one regime (4 binades) the fraction width is
-// fixed, so C = 2^e * G with G = 1.5 * 2^(52 - fb) the regime's gain, and 2^e is the sum
-// with its sign and fraction bits masked off: one AND and one FP64 multiply.  The fraction
-// width is that of the value a block of steps starts at; it is the same in regimes k and
-// -k-1 (both have a run of the same length), so the scales [2^-4, 2^4) around 1 form one
-// such range of 8 binades, and the other ranges are single regimes.  A step whose sum
-// lands at another fraction width (or is zero, or is risky as in f64_posit_add) is
-// flagged, and the caller redoes the block with chain_add_one.
-PG_HD double f64_regime_gain(int32_t k)
-{
-    const int32_t fb = 28 - ((k ^ (k >> 31)) + 1);
-    return f64_from_bits(((uint64_t)(uint32_t)(52 - fb + 1023) << 52) | 0x0008000000000000ull);
-}
-
+// operations on the dependent path.  Within a range of scales of one fraction width fb the
+// posit grid is every number with fb + 1 significant bits, so the rounding is that of the
+// FP64 significand to 53 - sh bits (sh = 52 - fb), to nearest, ties to even (the last
+// fraction bit is the pattern's), whatever the binade.  Veltkamp's splitting (Dekker, "A
+// floating-point technique for extending the available precision", 1971) does exactly
+// that in FP64 arithmetic rounded to nearest even: with C = 2^sh + 1, g = fl(C s),
+// d = fl(s - g), the high part fl(g + d) is s rounded to 53 - sh bits (2 <= sh <= 51), ties
+// to even.  So a step is s = fl(t + q) and three more FP64 operations, no exponent on the
+// dependent path.  The fraction width is that of the value a block of steps starts at; it
+// is the same in regimes k and -k-1 (both have a run of the same length), so the scales
+// [2^-4, 2^4) around 1 form one such range of 8 binades, and the other ranges are single
+// regimes.  A step whose sum lands at another fraction width (or is zero, or is risky as in
+// f64_posit_add) is flagged, and the caller redoes the block with chain_add_one.
 PG_HD int32_t f64_regime(double x) { return ((int32_t)((f64_bits(x) >> 52) & 0x7FF) - 1023) >> 2; }
 
 // The regime run length of the scale of FP64 pattern sb (fb = 28 - run).
@@ -337,13 +337,16 @@ PG_HD int32_t f64_bits_run(uint64_t sb)
     return (k ^ (k >> 31)) + 1;
 }
 
-PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t run, uint32_t &bad)
+// C = 2^sh + 1 for regime run `run` (sh = 52 - fb = 24 + run).
+PG_HD double f64_split_const(int32_t run) { return f64_add(f64_from_bits((uint64_t)(24 + run + 1023) << 52), 1.0); }
+
+PG_HD double f64_posit_add_split(double t, double q, double C, int32_t run, uint32_t &bad)
 {
     const double s = f64_add(t, q);
-    const uint64_t sb = f64_bits(s);
-    const double C = f64_mul(f64_from_bits(sb & 0x7FF0000000000000ull), G);
-    const double r = f64_add(f64_add(s, C), -C);
+    const double g = f64_mul(C, s);
+    const double r = f64_add(g, f64_add(s, -g));
     // off the dependent path
+    const uint64_t sb = f64_bits(s);
     const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
     const int32_t gap = et > eq ? et - eq : eq - et;
     const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
@@ -351,28 +354,7 @@ PG_HD double f64_posit_add_reg(double t, double q, double G, int32_t run, uint32
     return r;
 }
 
-// The same step with the rounding done on the FP64 pattern.  Within one regime the posit
-// keeps fb fraction bits in every binade, so rounding the exact sum s to the posit grid is
-// rounding its FP64 significand to fb bits, to nearest, ties to even: add 2^(sh-1) - 1
-// plus the last kept bit to the pattern's magnitude and clear the sh = 52 - fb bits below
-// (a carry out of the significand moves into the exponent, which is the correct result).
-// On the dependent path that is one FP64 addition and a few integer operations instead of
-// an AND, an FP64 multiply and two FP64 additions.  sh <= 31: the kept bit and the cleared
-// bits are in the low word.
-PG_HD double f64_posit_add_reg_int(double t, double q, uint32_t sh, int32_t run, uint32_t &bad)
-{
-    const double s = f64_add(t, q);
-    const uint64_t sb = f64_bits(s);
-    const uint64_t rb = (sb + (((uint64_t)1 << (sh - 1)) - 1) + ((sb >> sh) & 1)) & ~(((uint64_t)1 << sh) - 1);
-    // off the dependent path
-    const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
-    const int32_t gap = et > eq ? et - eq : eq - et;
-    const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
-    bad |= (risky | (f64_bits_run(sb) != run)) ? 0x40000000u : 0u;
-    return f64_from_bits(rb);
-}
-
-// t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-regime step: blocks of
+// t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-width step: blocks of
 // CHAIN_BLOCK steps without a branch, a flagged block redone step by step exactly.
 // Terms read from FP64 values or from posit32 patterns (converted on load).
 struct TermsF64 {
@@ -394,24 +376,17 @@ PG_HD double chain_add_run_reg(double t, Q q, int count)
     for (; k + U <= count; k += U) {
         const int32_t kreg = f64_regime(t);
         const bool in = (t != 0.0) & (kreg >= (FAST_LO >> 2)) & (kreg <= (FAST_HI >> 2));
-        const double G = f64_regime_gain(kreg);
+        const int32_t run = (kreg ^ (kreg >> 31)) + 1;
+        const double C = f64_split_const(run);
         double v[U];
 #pragma unroll
         for (int j = 0; j < U; ++j)
             v[j] = q[k + j];
         const double t0 = t;
         uint32_t bad = in ? 0u : 0x40000000u;
-        const int32_t run = (kreg ^ (kreg >> 31)) + 1; // fb = 28 - run
-        if (run <= 7) {                                 // sh = 24 + run <= 31
-            const uint32_t sh = 24u + (uint32_t)run;
 #pragma unroll
-            for (int j = 0; j < U; ++j)
-                t = f64_posit_add_reg_int(t, v[j], sh, run, bad);
-        } else {
-#pragma unroll
-            for (int j = 0; j < U; ++j)
-                t = f64_posit_add_reg(t, v[j], G, run, bad);
-        }
+        for (int j = 0; j < U; ++j)
+            t = f64_posit_add_split(t, v[j], C, run, bad);
         if (bad & 0x40000000u) { // (from q: a dynamic index into v would put v in local memory)
             t = t0;
             for (int j = 0; j < U; ++j)

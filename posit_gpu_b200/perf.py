@@ -41,19 +41,22 @@ def fp64_pipe_peak_warp_inst_per_s(sm_mhz):
 
 
 # The instruction count above belongs to one build of the main kernel.  It is tied to
-# that build by a SHA-256 over the sources that define the kernel's instruction stream and
-# the script that compiles them (flags included); the benchmark recomputes the digest and,
-# when it differs, marks the count stale and reports no roofline fraction from it.
-KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh", "build.py"]
-INST_SOURCE_DIGEST = "0655770ff12d388eae556ca0a5c2fff79a0e8127ce0e6905dc3606f40832bf51"
+# that build by a SHA-256 over the sources that define the kernel's instruction stream
+# (gemm.cu and the headers it includes) and the compiler flags (build.py's ARCH and CFLAGS);
+# the benchmark recomputes the digest and, when it differs, marks the count stale and
+# reports no roofline fraction from it.
+KERNEL_SOURCES = ["csrc/gemm.cu", "csrc/gemm.cuh", "csrc/gemm_tile.cuh", "csrc/posit32.cuh"]
+INST_SOURCE_DIGEST = "5a203b78e19bc143f412235179eae4c1e55abcb0a85c594a21c4e0e78f9bed8d"
 
 
 def kernel_source_digest():
+    from . import build as _build
     here = os.path.dirname(os.path.abspath(__file__))
     h = hashlib.sha256()
     for rel in KERNEL_SOURCES:
         with open(os.path.join(here, rel), "rb") as fh:
             h.update(rel.encode() + b"\0" + fh.read() + b"\0")
+    h.update(b"flags\0" + " ".join(_build.ARCH + _build.CFLAGS).encode() + b"\0")
     return h.hexdigest()
 
 

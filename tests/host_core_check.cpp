@@ -2,6 +2,7 @@
 // CPU tests against the oracle.  Compiled by tests/test_posit_core_cpu.py.
 #include "../posit_gpu_b200/csrc/posit32.cuh"
 #include "../posit_gpu_b200/csrc/trsm_chain.cuh"
+#include "../posit_gpu_b200/csrc/posit32_div.cuh"
 #include <stdint.h>
 #include <algorithm>
 #include <vector>
@@ -11,6 +12,8 @@ void hc_pmul_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for 
 void hc_padd_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = padd(a[i], b[i]); }
 void hc_pdiv_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = pdiv(a[i], b[i]); }
 void hc_psqrt_n(const uint32_t *a, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = psqrt(a[i]); }
+void hc_pdiv_est_n(const uint32_t *a, const uint32_t *b, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = pdiv_est(a[i], b[i]); }
+void hc_psqrt_est_n(const uint32_t *a, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = psqrt_est(a[i]); }
 void hc_from_double_n(const double *x, uint32_t *o, long n) { for (long i = 0; i < n; i++) o[i] = p32_from_double(x[i]); }
 // c + t*a through the decoded integer form (computed regime entries, exact fallback), as
 // llt_chain runs it; counts the steps the fast path did alone
@@ -286,6 +289,37 @@ long hc_from_double_exact_mismatch(const uint32_t *u, long n)
     long bad = 0;
     for (long i = 0; i < n; i++)
         bad += p32_from_double_exact(p32_to_double(u[i])) != u[i];
+    return bad;
+}
+// Veltkamp's split (the high part of (2^sh+1)s) against rounding the FP64 significand to
+// 53 - sh bits with integer operations (nearest, ties to even), for sh = 25..51 on n random
+// values per sh, a third of them exact ties and a third one unit either side of a tie.
+// Returns the number of mismatches.
+long hc_split_round_check(uint64_t seed, long n)
+{
+    uint64_t st = seed | 1;
+    auto rnd = [&]() { st ^= st << 13; st ^= st >> 7; st ^= st << 17; return st; };
+    long bad = 0;
+    for (int sh = 25; sh <= 51; ++sh) {
+        const double C = f64_add(f64_from_bits((uint64_t)(sh + 1023) << 52), 1.0);
+        const uint64_t half = (uint64_t)1 << (sh - 1), low = ((uint64_t)1 << sh) - 1;
+        for (long i = 0; i < n; ++i) {
+            uint64_t m = rnd() & 0xFFFFFFFFFFFFFull;
+            const uint64_t kind = rnd() % 4;
+            if (kind == 0)
+                m = (m & ~low) | half;
+            else if (kind == 1)
+                m = (m & ~low) | (half + 1);
+            else if (kind == 2)
+                m = (m & ~low) | (half - 1);
+            const uint64_t b = ((rnd() & 1) << 63) | ((uint64_t)(1023 + (int)(rnd() % 241) - 120) << 52) | m;
+            const double s = f64_from_bits(b);
+            const uint64_t want = (b + (half - 1) + ((b >> sh) & 1)) & ~low;
+            const double g = f64_mul(C, s);
+            const double r = f64_add(g, f64_add(s, -g));
+            bad += f64_bits(r) != want;
+        }
+    }
     return bad;
 }
 // chain_add_run_reg against chain_add_run on one chain of n terms (patterns); 1 on a match

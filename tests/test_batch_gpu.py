@@ -40,15 +40,21 @@ def test_batch_matches_oracle_and_per_call(cuda_ok):
     for n in (1, 2, 5, 8, 17, 31, 64, 100, 130, 257, 300):
         for kind in (0, 1):
             specs.append((kind, n, int(rng.integers(1, 5))))
-    # a singular LU and a non-positive-definite Cholesky
-    specs += [(0, 40, 2), (1, 45, 1)]
+    # a singular LU, a non-positive-definite Cholesky, and an LU whose first column is NaR
+    # over zeros (a zero pivot below the diagonal: rows 0 and 1 trade places in every
+    # column but the first)
+    specs += [(0, 40, 2), (1, 45, 1), (0, 40, 2)]
     host = [_problem(rng, k, n, r) for (k, n, r) in specs]
-    A0 = host[-2][0].reshape(40, 40, order="F")
+    A0 = host[-3][0].reshape(40, 40, order="F")
     A0[:, 7] = 0
-    host[-2] = (np.ascontiguousarray(A0.reshape(-1, order="F")), host[-2][1])
-    S0 = host[-1][0].reshape(45, 45, order="F")
+    host[-3] = (np.ascontiguousarray(A0.reshape(-1, order="F")), host[-3][1])
+    S0 = host[-2][0].reshape(45, 45, order="F")
     S0[30, 30] = oracle.p32(-2.0)
-    host[-1] = (np.ascontiguousarray(S0.reshape(-1, order="F")), host[-1][1])
+    host[-2] = (np.ascontiguousarray(S0.reshape(-1, order="F")), host[-2][1])
+    A1 = host[-1][0].reshape(40, 40, order="F")
+    A1[:, 0] = 0
+    A1[0, 0] = oracle.P32_NAR
+    host[-1] = (np.ascontiguousarray(A1.reshape(-1, order="F")), host[-1][1])
     dev = torch.device("cuda")
     tens = []
     for (kind, n, r), (A, B) in zip(specs, host):

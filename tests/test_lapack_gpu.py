@@ -55,6 +55,26 @@ def test_rgetrf_singular_and_zero_pivots(cuda_ok):
     assert np.array_equal(pg_, po) and np.array_equal(g, o)
 
 
+@pytest.mark.parametrize("m,n", [(80, 80), (3000, 40)])
+def test_rgetrf_zero_pivot_below_a_nar_row(cuda_ok, m, n):
+    """Column 0 is NaR on the diagonal and zero below: iRamax takes the first zero (row 1),
+    the pivot is zero, so no interchange happens and u comes from row 0 (the NaR row);
+    info is 1.  One panel CTA (m = 80) and a cluster of three (m = 3000)."""
+    import posit_gpu_b200 as pg
+    rng = np.random.default_rng(m + 7)
+    A = _ge(rng, m, n).reshape(m, n, order="F")
+    A[:, 0] = 0
+    A[0, 0] = oracle.P32_NAR
+    A = np.ascontiguousarray(A.reshape(-1, order="F"))
+    g, o = A.copy(), A.copy()
+    pg_, po = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    info_g = pg.Rgetrf(m, n, g, m, pg_, 16)
+    info_o = oracle.orc.orc_rgetrf(m, n, o, m, po, 16)
+    assert info_g == info_o == 1
+    assert pg_[0] == po[0] == 2
+    assert np.array_equal(pg_, po) and np.array_equal(g, o)
+
+
 @pytest.mark.parametrize("n,nrhs", [(1, 1), (7, 3), (150, 5), (513, 16)])
 def test_rgetrs_bit_exact(cuda_ok, n, nrhs):
     import posit_gpu_b200 as pg
@@ -82,15 +102,17 @@ def test_rpotrf_lower_bit_exact(cuda_ok, n, nb):
     assert np.array_equal(g, o)
 
 
-def test_rpotrf_not_positive_definite(cuda_ok):
+@pytest.mark.parametrize("n,bad", [(120, 77), (700, 20)])
+def test_rpotrf_not_positive_definite(cuda_ok, n, bad):
+    """The leading minor of order bad+1 fails: in a later one-CTA panel (n = 120) or in the
+    first panel, held by a cluster of six CTAs (n = 700)."""
     import posit_gpu_b200 as pg
     rng = np.random.default_rng(9)
-    n = 120
     S = _spd(rng, n).reshape(n, n, order="F")
-    S[77, 77] = oracle.p32(-1.0)  # the leading minor of order 78 fails
+    S[bad, bad] = oracle.p32(-1.0)
     S = np.ascontiguousarray(S.reshape(-1, order="F"))
     g, o = S.copy(), S.copy()
-    assert pg.Rpotrf("L", n, g, n, 32) == oracle.orc.orc_rpotrf(b"L", n, o, n, 32) > 0
+    assert pg.Rpotrf("L", n, g, n, 32) == oracle.orc.orc_rpotrf(b"L", n, o, n, 32) == bad + 1
 
 
 @pytest.mark.parametrize("n,nrhs", [(1, 1), (9, 2), (200, 4), (400, 16)])

@@ -23,9 +23,10 @@ def hc(tmp_path_factory):
     subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", str(out),
                            os.path.join(HERE, "host_core_check.cpp")])
     lib = ctypes.CDLL(str(out))
-    for nm in ("hc_pmul_n", "hc_padd_n", "hc_pdiv_n"):
+    for nm in ("hc_pmul_n", "hc_padd_n", "hc_pdiv_n", "hc_pdiv_est_n"):
         getattr(lib, nm).argtypes = [U32, U32, U32, ctypes.c_long]
     lib.hc_psqrt_n.argtypes = [U32, U32, ctypes.c_long]
+    lib.hc_psqrt_est_n.argtypes = [U32, U32, ctypes.c_long]
     lib.hc_from_double_n.argtypes = [F64, U32, ctypes.c_long]
     lib.hc_dmac_n.argtypes = [U32, U32, U32, U32, ctypes.c_long]
     lib.hc_dmac_n.restype = ctypes.c_long
@@ -79,6 +80,35 @@ def test_pattern_ops_match_oracle(hc):
     o1, o2 = np.empty_like(a), np.empty_like(a)
     hc.hc_psqrt_n(a, o1, a.size)
     oracle.orc.orc_p32_sqrt_n(a, o2, a.size)
+    assert np.array_equal(o1, o2)
+
+
+def test_division_and_root_from_fp64_estimates_match_oracle(hc):
+    """pdiv_est / psqrt_est (the integer quotient and root from one FP64 division or square
+    root, corrected by the exact remainder) equal p32_div / p32_sqrt on mixed patterns, on
+    exact quotients (a = b, a = b*c with small c, powers of two), on every significand
+    pattern with a fixed scale (square roots near the top and bottom of their binades), and
+    on the extremes."""
+    rng = np.random.default_rng(11)
+    a, b = _mix(rng, 400_000), _mix(rng, 400_000)
+    small = oracle.from_double(rng.choice([1.0, 2.0, 3.0, 0.5, 0.75, 1.5, 5.0, 7.0, 0.125], 100_000))
+    b2 = _mix(rng, 100_000)
+    a2 = np.empty_like(b2)
+    oracle.orc.orc_p32_mul_n(b2, small, a2, b2.size)
+    a = np.concatenate([a, a2, b2, b2 ^ np.uint32(0x80000000)])
+    b = np.concatenate([b, b2, b2, b2])
+    o1, o2 = np.empty_like(a), np.empty_like(a)
+    hc.hc_pdiv_est_n(a, b, o1, a.size)
+    oracle.orc.orc_p32_div_n(a, b, o2, a.size)
+    assert np.array_equal(o1, o2)
+    # square roots: random patterns, every fraction of the binades [1, 4) and [2^-40, 2^-38)
+    fr = np.arange(0, 1 << 22, dtype=np.uint32)
+    sq = np.concatenate([_mix(rng, 400_000), 0x40000000 + (fr << 5), 0x40000000 - (fr << 5),
+                         np.array([1, 2, 3, 0x7FFFFFFF, 0x7FFFFFFE, 0x40000000, 0x3FFFFFFF], np.uint32)])
+    sq = np.ascontiguousarray(sq)
+    o1, o2 = np.empty_like(sq), np.empty_like(sq)
+    hc.hc_psqrt_est_n(sq, o1, sq.size)
+    oracle.orc.orc_p32_sqrt_n(sq, o2, sq.size)
     assert np.array_equal(o1, o2)
 
 
@@ -368,6 +398,15 @@ def test_scan_form_of_the_chain_matches_sequential_additions(hc):
         assert hc.hc_scan_row_check(c0, np.ascontiguousarray(q), n, E, stats) == 1, (trial, kind, n, E)
         assert hc.hc_chain_reg_check(c0, np.ascontiguousarray(q), n) == 1, (trial, kind, n, "reg")
     assert stats[0] > 0 and stats[1] > 0  # both scans and exact steps were exercised
+
+
+def test_split_rounding_is_nearest_even_at_every_width(hc):
+    """Veltkamp's split in FP64 (the fixed-width chain step's rounding: the high part of
+    (2^sh+1)s) equals rounding the significand to 53 - sh bits, nearest, ties to even, for
+    every shift the posit fraction widths need, on exact ties and their neighbours."""
+    hc.hc_split_round_check.restype = ctypes.c_long
+    hc.hc_split_round_check.argtypes = [ctypes.c_uint64, ctypes.c_long]
+    assert hc.hc_split_round_check(20261204, 200_000) == 0
 
 
 def test_exact_encode_round_trips_every_pattern_class(hc):
