@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--batch-max-n", type=int, default=0, help="serve: batched-kernel size limit (0: default)")
     ap.add_argument("--lanes", type=int, default=0, help="serve: CUDA streams of the server (0: default)")
     ap.add_argument("--launch-threads", type=int, default=0, help="serve: launcher threads (0: default)")
+    ap.add_argument("--serve-nb", type=int, default=0, help="serve: the server's panel width (0: its default)")
+    ap.add_argument("--serve-priority-n", type=int, default=0,
+                    help="serve: n from which requests run on high-priority lanes (0: default, -1: none)")
     ap.add_argument("--profile-path", default="", choices=["", "percall", "served"],
                     help="serve: bracket only this path with cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off); both paths still run")
@@ -804,7 +807,8 @@ def serve_arm(args):
         arng = np.random.default_rng(77)
         gaps = np.zeros(R) if rate == "burst" else arng.exponential(1.0 / float(rate), R)
         arrive = np.cumsum(gaps) - gaps[0]
-        with pg.Server(batch_max_n=args.batch_max_n, lanes=args.lanes, launch_threads=args.launch_threads) as srv:
+        with pg.Server(batch_max_n=args.batch_max_n, lanes=args.lanes, launch_threads=args.launch_threads,
+                       nb=args.serve_nb, priority_n=args.serve_priority_n) as srv:
             tickets, t_sub = [None] * R, [0.0] * R
 
             def feed():
@@ -866,7 +870,9 @@ def serve_arm(args):
             "vs_baseline": None, "dtype": "posit32", "data": "synthetic",
             "config": {"workload": f"config 5: {R} requests, 50% LU / 50% Cholesky(L), {repeats} repeat "
                                    "matrices (30%), B = A*X_true, Poisson arrivals per rate, 150 GB budget",
-                       "rates": rates, "batch_max_n": args.batch_max_n or 256},
+                       "rates": rates, "batch_max_n": args.batch_max_n or 256,
+                       "server_nb": args.serve_nb or "max(32, tuned) per n",
+                       "server_priority_n": args.serve_priority_n or "default (2048)"},
             "e2e": {"value": best["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": round(h2d),
                     "d2h_bytes_per_step": round(sum(4 * q[1] * q[2] for q in reqs) / R),
                     "note": "value is itself end to end: host buffers in, solution in host memory"},

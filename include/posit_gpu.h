@@ -191,6 +191,7 @@ void posit_batch_plan_destroy(posit_batch_plan *plan);
 #define POSIT_E_MISMATCH (-11)       /* matrix_id cached with another kind or n */
 #define POSIT_E_UNKNOWN_TICKET (-12) /* no such ticket (or its result was already taken) */
 #define POSIT_SERVER_DEFAULT_BUDGET ((size_t)150000000000ull) /* 150 GB */
+#define POSIT_SERVER_PRIORITY_N 2048
 typedef struct posit_server posit_server;
 typedef struct {
     size_t memory_budget; /* device bytes; 0 = 150 GB (capped at free memory - 2 GiB) */
@@ -199,11 +200,16 @@ typedef struct {
     int lanes;            /* CUDA streams work units run on; 0 = 64 */
     int launch_threads;   /* threads issuing the units' CUDA work; 0 = 8 */
     int batch_max_n;      /* n <= this goes to the batched kernel; 0 = 256 (max POSIT_BATCH_MAX_N) */
-    int nb;               /* panel width of the blocked path; 0 = the tuned width for each n */
+    int nb;               /* panel width of the blocked path; 0 = the tuned width for each n, at
+                             least 32 (wider panels serve more requests per second when many
+                             share the GPU; the bits do not depend on nb) */
     int cache_off;        /* 1: never keep factors */
     int batch_lanes;      /* lanes reserved for batched units; 0 = 4 */
     int order_window_ms;  /* > 0: requests submitted within one window of this many ms are
                              admitted largest work first, windows in arrival order; 0 = arrival order */
+    int priority_n;       /* blocked requests with n >= this run on lanes of the device's greatest
+                             stream priority (a quarter of the blocked lanes), so the longest
+                             requests get SMs first; 0 = POSIT_SERVER_PRIORITY_N, < 0 = none */
 } posit_server_config;
 typedef struct {
     int kind;             /* POSIT_BATCH_LU or POSIT_BATCH_CHOLESKY (lower) */

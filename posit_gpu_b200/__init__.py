@@ -372,7 +372,8 @@ def profile_read(reset=True):
 class _ServerConfig(_c.Structure):
     _fields_ = [("memory_budget", _c.c_size_t), ("max_inflight", _c.c_int), ("max_queue", _c.c_int),
                 ("lanes", _c.c_int), ("launch_threads", _c.c_int), ("batch_max_n", _c.c_int), ("nb", _c.c_int),
-                ("cache_off", _c.c_int), ("batch_lanes", _c.c_int), ("order_window_ms", _c.c_int)]
+                ("cache_off", _c.c_int), ("batch_lanes", _c.c_int), ("order_window_ms", _c.c_int),
+                ("priority_n", _c.c_int)]
 
 
 class _SolveRequest(_c.Structure):
@@ -433,9 +434,9 @@ class Server:
     """
 
     def __init__(self, memory_budget=0, max_inflight=0, max_queue=0, lanes=0, launch_threads=0,
-                 batch_max_n=0, nb=0, cache=True, batch_lanes=0, order_window_ms=0):
+                 batch_max_n=0, nb=0, cache=True, batch_lanes=0, order_window_ms=0, priority_n=0):
         cfg = _ServerConfig(int(memory_budget), max_inflight, max_queue, lanes, launch_threads, batch_max_n, nb,
-                            0 if cache else 1, batch_lanes, order_window_ms)
+                            0 if cache else 1, batch_lanes, order_window_ms, priority_n)
         h = _VP()
         _check(_lib.posit_server_create(_c.byref(cfg), _c.byref(h)), "server")
         self._h = h

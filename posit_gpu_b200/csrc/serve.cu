@@ -97,6 +97,7 @@ struct Lane {
     std::vector<void *> retired; // outgrown page-locked buffers (freed at shutdown)
     bool busy = false;           // loop thread only
     bool for_batches = false;    // reserved for batched units
+    bool high = false;           // created with the device's greatest stream priority
 };
 
 struct Unit {
@@ -113,7 +114,7 @@ struct Unit {
 struct posit_server {
     // configuration
     size_t budget = 0;
-    int max_inflight = 0, max_queue = 0, batch_max_n = 0, nb = 0;
+    int max_inflight = 0, max_queue = 0, batch_max_n = 0, nb = 0, priority_n = 0;
     double order_window_ms = 0.0; // 0: arrival order
     bool cache_on = true;
     int device = 0, sms = 148;
@@ -152,10 +153,16 @@ struct posit_server {
 
 namespace {
 
-// Panel width of a blocked unit: the configured one, or the tuned width for its n.
+// Panel width of a blocked unit: the configured one, or the tuned width for its n but at
+// least SERVE_MIN_NB.  The tuned widths minimise one factorization's time alone; with many
+// units sharing the GPU the panels' latency hides behind other units and the trailing
+// GEMMs' efficiency counts (k = 16 runs at 64 % of k = 256's rate), so wider panels serve
+// more requests per second (the serving burst: 656 solves/s at nb = 32 against 567 at the
+// tuned 16, 523 at 64, 457 at 128).  The bits do not depend on nb.
+constexpr int SERVE_MIN_NB = 32;
 int serve_nb(const posit_server *s, int kind, int n)
 {
-    return s->nb > 0 ? s->nb : pg::tuned_panel_width(kind == POSIT_BATCH_LU, n);
+    return s->nb > 0 ? s->nb : std::max(SERVE_MIN_NB, pg::tuned_panel_width(kind == POSIT_BATCH_LU, n));
 }
 
 size_t ws_bytes(const posit_server *s, int kind, int n)
@@ -516,10 +523,12 @@ void admit(posit_server *s, std::vector<Req> &done, std::vector<Unit *> &units)
     order_pending(s);
     // Lanes reserved for batched units keep small requests from waiting behind long
     // blocked ones; a batched unit may also take a free blocked lane.
-    std::vector<Lane *> idle_batch, idle_blocked;
+    // Blocked lanes: those of the greatest priority take the requests of n >= priority_n
+    // first; either kind takes the other's lanes when its own are busy.
+    std::vector<Lane *> idle_batch, idle_hi, idle_lo;
     for (auto &L : s->lanes)
         if (!L.busy)
-            (L.for_batches ? idle_batch : idle_blocked).push_back(&L);
+            (L.for_batches ? idle_batch : (L.high ? idle_hi : idle_lo)).push_back(&L);
     Unit *group = nullptr;
     bool small_waits = false, large_waits = false; // no lane: later ones of that kind wait too
     auto drop = [&](std::deque<Req>::iterator it) {
@@ -561,10 +570,11 @@ void admit(posit_server *s, std::vector<Req> &done, std::vector<Unit *> &units)
             break;
         const bool hit = f != nullptr;
         const bool small = q.n <= s->batch_max_n;
+        const bool none_blocked = idle_hi.empty() && idle_lo.empty();
         if (small) {
-            small_waits |= !group && idle_batch.empty() && idle_blocked.empty();
+            small_waits |= !group && idle_batch.empty() && none_blocked;
         } else {
-            large_waits |= idle_blocked.empty();
+            large_waits |= none_blocked;
         }
         if (small ? small_waits : large_waits) {
             ++it;
@@ -610,7 +620,7 @@ void admit(posit_server *s, std::vector<Req> &done, std::vector<Unit *> &units)
                 group = new Unit();
                 group->srv = s;
                 group->batched = true;
-                auto &from = idle_batch.empty() ? idle_blocked : idle_batch;
+                auto &from = !idle_batch.empty() ? idle_batch : (!idle_lo.empty() ? idle_lo : idle_hi);
                 group->lane = from.back();
                 from.pop_back();
             }
@@ -618,8 +628,10 @@ void admit(posit_server *s, std::vector<Req> &done, std::vector<Unit *> &units)
         } else {
             Unit *u = new Unit();
             u->srv = s;
-            u->lane = idle_blocked.back();
-            idle_blocked.pop_back();
+            const bool prio = s->priority_n > 0 && q.n >= s->priority_n;
+            auto &from = prio ? (!idle_hi.empty() ? idle_hi : idle_lo) : (!idle_lo.empty() ? idle_lo : idle_hi);
+            u->lane = from.back();
+            from.pop_back();
             u->reqs.push_back(r);
             u->extra_bytes = ws;
             units.push_back(u);
@@ -748,7 +760,8 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
     s->max_inflight = c.max_inflight > 0 ? c.max_inflight : 4096;
     s->max_queue = c.max_queue > 0 ? c.max_queue : (1 << 20);
     s->batch_max_n = c.batch_max_n > 0 ? std::min(c.batch_max_n, POSIT_BATCH_MAX_N) : 256;
-    s->nb = c.nb > 0 ? c.nb : 0; // 0: the tuned width for each request's n
+    s->nb = c.nb > 0 ? c.nb : 0; // 0: the server's width for each request's n (serve_nb)
+    s->priority_n = c.priority_n < 0 ? 0 : (c.priority_n > 0 ? c.priority_n : POSIT_SERVER_PRIORITY_N);
     s->order_window_ms = c.order_window_ms > 0 ? (double)c.order_window_ms : 0.0;
     s->cache_on = c.cache_off == 0;
     const int nlanes = std::max(2, c.lanes > 0 ? c.lanes : 64);
@@ -768,10 +781,16 @@ int posit_server_create(const posit_server_config *cfg, posit_server **out)
         e = cudaStreamCreateWithFlags(&s->free_st, cudaStreamNonBlocking);
     if (e == cudaSuccess)
         e = pg::device_error_address(&s->d_err);
+    int prio_least = 0, prio_greatest = 0;
+    if (e == cudaSuccess)
+        e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    const int nhigh = s->priority_n > 0 ? std::max(1, (nlanes - nbatch) / 4) : 0;
     s->lanes.resize(nlanes);
     for (int i = 0; i < nlanes && e == cudaSuccess; ++i) {
-        s->lanes[i].for_batches = i < nbatch;
-        e = cudaStreamCreateWithFlags(&s->lanes[i].st, cudaStreamNonBlocking);
+        Lane &L = s->lanes[i];
+        L.for_batches = i < nbatch;
+        L.high = !L.for_batches && i >= nlanes - nhigh;
+        e = cudaStreamCreateWithPriority(&L.st, cudaStreamNonBlocking, L.high ? prio_greatest : prio_least);
     }
     if (e != cudaSuccess) {
         shutdown_resources(s);
