@@ -326,8 +326,8 @@ PG_HD double chain_add_one(double t, double q)
 // dependent path.  The fraction width is that of the value a block of steps starts at; it
 // is the same in regimes k and -k-1 (both have a run of the same length), so the scales
 // [2^-4, 2^4) around 1 form one such range of 8 binades, and the other ranges are single
-// regimes.  A block with a step whose sum lands at another fraction width (or is zero, or
-// is risky as in f64_posit_add) is redone with chain_add_one.
+// regimes.  A step whose sum lands at another fraction width (or is zero, or is risky as in
+// f64_posit_add) is flagged, and the caller redoes the block with chain_add_one.
 PG_HD int32_t f64_regime(double x) { return ((int32_t)((f64_bits(x) >> 52) & 0x7FF) - 1023) >> 2; }
 
 // The regime run length of the scale of FP64 pattern sb (fb = 28 - run).
@@ -340,40 +340,23 @@ PG_HD int32_t f64_bits_run(uint64_t sb)
 // C = 2^sh + 1 for regime run `run` (sh = 52 - fb = 24 + run).
 PG_HD double f64_split_const(int32_t run) { return f64_add(f64_from_bits((uint64_t)(24 + run + 1023) << 52), 1.0); }
 
-// s rounded to the fraction width of C (Veltkamp's high part).
-PG_HD double f64_split_round(double s, double C)
+PG_HD double f64_posit_add_split(double t, double q, double C, int32_t run, uint32_t &bad)
 {
+    const double s = f64_add(t, q);
     const double g = f64_mul(C, s);
-    return f64_add(g, f64_add(s, -g));
-}
-
-// Is the split step t + q = s one the fixed-width form does exactly?  Not when the operands
-// are 25..30 binades apart (as in f64_posit_add) or the sum lies at another fraction width
-// (zero and the scales outside the fast window included).
-PG_HD bool f64_split_step_ok(double t, double q, double s, int32_t run)
-{
+    const double r = f64_add(g, f64_add(s, -g));
+    // off the dependent path
+    const uint64_t sb = f64_bits(s);
     const int32_t et = (int32_t)((f64_bits(t) >> 52) & 0x7FF), eq = (int32_t)((f64_bits(q) >> 52) & 0x7FF);
     const int32_t gap = et > eq ? et - eq : eq - et;
     const bool risky = (eq != 0) & (gap > 24) & (gap <= 30);
-    return !risky & (f64_bits_run(f64_bits(s)) == run);
-}
-
-// The fraction width (as the regime run) a block starting at t uses; 0 when t is zero or
-// outside the fast window (no fixed-width block then).
-PG_HD int32_t f64_block_run(double t)
-{
-    const int32_t kreg = f64_regime(t);
-    const bool in = (t != 0.0) & (kreg >= (FAST_LO >> 2)) & (kreg <= (FAST_HI >> 2));
-    return in ? (kreg ^ (kreg >> 31)) + 1 : 0;
+    bad |= (risky | (f64_bits_run(sb) != run)) ? 0x40000000u : 0u;
+    return r;
 }
 
 // t + q_0 + ... + q_{count-1} as chain_add_run, with the fixed-width step: blocks of
-// CHAIN_BLOCK steps without a branch, each step four dependent FP64 operations.  Nothing
-// else is on the dependent path: the width (and C) carry over from block to block, a block
-// checks afterwards that its start value had that width and that every step was one the
-// form does exactly (from the saved operands and sums), and a block that fails is redone
-// step by step exactly, after which the width is taken afresh.  Terms read from FP64
-// values or from posit32 patterns (converted on load).
+// CHAIN_BLOCK steps without a branch, a flagged block redone step by step exactly.
+// Terms read from FP64 values or from posit32 patterns (converted on load).
 struct TermsF64 {
     const double *q;
     PG_HD_MEMBER double operator[](int i) const { return q[i]; }
@@ -390,30 +373,24 @@ PG_HD double chain_add_run_reg(double t, Q q, int count)
 {
     constexpr int U = CHAIN_BLOCK;
     int k = 0;
-    int32_t run = f64_block_run(t);
-    double C = f64_split_const(run > 0 ? run : 1);
     for (; k + U <= count; k += U) {
-        double v[U], tv[U], sv[U];
+        const int32_t kreg = f64_regime(t);
+        const bool in = (t != 0.0) & (kreg >= (FAST_LO >> 2)) & (kreg <= (FAST_HI >> 2));
+        const int32_t run = (kreg ^ (kreg >> 31)) + 1;
+        const double C = f64_split_const(run);
+        double v[U];
 #pragma unroll
         for (int j = 0; j < U; ++j)
             v[j] = q[k + j];
         const double t0 = t;
-#pragma unroll
-        for (int j = 0; j < U; ++j) {
-            tv[j] = t;
-            sv[j] = f64_add(t, v[j]);
-            t = f64_split_round(sv[j], C);
-        }
-        bool ok = (run > 0) & (f64_block_run(t0) == run);
+        uint32_t bad = in ? 0u : 0x40000000u;
 #pragma unroll
         for (int j = 0; j < U; ++j)
-            ok &= f64_split_step_ok(tv[j], v[j], sv[j], run);
-        if (!ok) { // (from q: a dynamic index into v would put v in local memory)
+            t = f64_posit_add_split(t, v[j], C, run, bad);
+        if (bad & 0x40000000u) { // (from q: a dynamic index into v would put v in local memory)
             t = t0;
             for (int j = 0; j < U; ++j)
                 t = chain_add_one(t, q[k + j]);
-            run = f64_block_run(t);
-            C = f64_split_const(run > 0 ? run : 1);
         }
     }
     for (; k < count; ++k)
