@@ -600,10 +600,11 @@ __global__ void trsm_lun_kernel(const uint32_t *__restrict__ U, size_t ldu, uint
 }
 
 // The same two solves with the column staged in shared memory and each thread's rows of
-// the triangle's next column (and the next diagonal) loaded into registers while the
-// current step runs, so no step waits for memory: rows tid + j*T (j < J) belong to thread
-// tid.  The division's result b_k is stored at the start of the next step (every thread has
-// read b_k before the step's barrier), so a step has one barrier.
+// the triangle's next column loaded into registers while the current step runs, so no step
+// waits for memory: rows tid + j*T (j < J) belong to thread tid.  The thread that holds the
+// next step's row divides it by its diagonal right after that row's last update, before the
+// step's barrier, so every thread reads b_k already divided: one division per step instead
+// of one per thread, and one barrier per step.
 template <bool UPPER, int J>
 __global__ void __launch_bounds__(1024) trsm_col_kernel(const uint32_t *__restrict__ A, size_t lda,
                                                         uint32_t *__restrict__ B, size_t ldb, int m, bool unit,
@@ -617,25 +618,27 @@ __global__ void __launch_bounds__(1024) trsm_col_kernel(const uint32_t *__restri
     for (int i = tid; i < m; i += T)
         s_x[i] = p32_to_double(bcol[i]);
     auto step_col = [&](int st) { return UPPER ? m - 1 - st : st; };
-    uint32_t lc[J], ln[J];
-    uint32_t dc = 0, dn = 0;
-    {
-        const int k = step_col(0);
+    uint32_t lc[J], ln[J]; // this thread's rows of the current / next column
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-            const int i = tid + j * T;
-            lc[j] = i < m ? A[i + (size_t)k * lda] : 0u;
-        }
-        if (!unit)
-            dc = A[k + (size_t)k * lda];
+    for (int j = 0; j < J; ++j) {
+        const int i = tid + j * T;
+        lc[j] = i < m ? A[i + (size_t)step_col(0) * lda] : 0u;
     }
+    // b_i / a_ii by the thread holding row i (Rtrsm.cpp:127, 145; b_i = 0 is left alone, as
+    // the reference skips it)
+    auto finish = [&](int i, uint32_t d) {
+        const double v = s_x[i];
+        if (!unit && v != 0.0)
+            s_x[i] = p32_to_double(pdiv_est(p32_from_double_exact(v), d));
+    };
+    uint32_t dn = unit ? 0u : A[step_col(0) + (size_t)step_col(0) * lda];
+    __syncthreads(); // the column is staged
+    if (tid == step_col(0) % T)
+        finish(step_col(0), dn);
     __syncthreads();
-    int pend_k = -1; // thread 0: b_k divided in the last step, stored at the start of this one
-    double pend_v = 0.0;
     for (int st = 0; st < m; ++st) {
-        const int k = step_col(st);
+        const int k = step_col(st), kn = step_col(st + 1);
         if (st + 1 < m) {
-            const int kn = step_col(st + 1);
 #pragma unroll
             for (int j = 0; j < J; ++j) {
                 const int i = tid + j * T;
@@ -644,19 +647,8 @@ __global__ void __launch_bounds__(1024) trsm_col_kernel(const uint32_t *__restri
             if (!unit)
                 dn = A[kn + (size_t)kn * lda];
         }
-        if (pend_k >= 0) {
-            s_x[pend_k] = pend_v;
-            pend_k = -1;
-        }
-        double bk = s_x[k];
-        if (bk != 0.0) { // zero multipliers skipped (Rtrsm.cpp:125-126, 143-144)
-            if (!unit) {
-                bk = p32_to_double(pdiv_est(p32_from_double_exact(bk), dc));
-                if (tid == 0) {
-                    pend_k = k;
-                    pend_v = bk;
-                }
-            }
+        const double bk = s_x[k]; // final: divided by its row's thread at the end of the last step
+        if (bk != 0.0) {          // zero multipliers skipped (Rtrsm.cpp:125-126, 143-144)
             const double nb = -bk;
 #pragma unroll
             for (int j = 0; j < J; ++j) {
@@ -665,15 +657,14 @@ __global__ void __launch_bounds__(1024) trsm_col_kernel(const uint32_t *__restri
                     s_x[i] = trsm_update(s_x[i], nb, p32_to_double(lc[j]));
             }
         }
+        // the next step's row has had its last update: its thread divides it now
+        if (st + 1 < m && tid == kn % T)
+            finish(kn, dn);
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < J; ++j)
             lc[j] = ln[j];
-        dc = dn;
     }
-    if (pend_k >= 0)
-        s_x[pend_k] = pend_v;
-    __syncthreads();
     for (int i = tid; i < m; i += T)
         bcol[i] = p32_from_double_exact(s_x[i]);
 }
