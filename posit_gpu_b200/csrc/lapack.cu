@@ -1320,11 +1320,12 @@ size_t rgetrf_workspace_bytes(int m, int n, int nb)
 struct PanelForm {
     int ncta, R, T; // CTAs (0: the panel does not fit), slots per thread, threads per CTA
 };
-static PanelForm panel_form(int M, int jb)
+static PanelForm panel_form(int M, int jb, int max_ctas)
 {
     if (jb > PANEL1_MAX_JB)
         return {0, 0, 0};
-    const int ncta = std::max(1, std::min(PANEL1_MAX_CTAS, (M + PANEL1_ROWS_PER_CTA - 1) / PANEL1_ROWS_PER_CTA));
+    const int cap = max_ctas > 0 ? std::min(max_ctas, PANEL1_MAX_CTAS) : PANEL1_MAX_CTAS;
+    const int ncta = std::max(1, std::min(cap, (M + PANEL1_ROWS_PER_CTA - 1) / PANEL1_ROWS_PER_CTA));
     const int rpc = (M + ncta - 1) / ncta; // rows per CTA
     const int T = std::min(PANEL1_THREADS, (rpc + 31) / 32 * 32), R = (rpc + T - 1) / T;
     if ((size_t)R * jb * T > (size_t)PANEL1_SMEM_ENTRIES * PANEL1_THREADS || R > PANEL1_MAX_R)
@@ -1364,7 +1365,7 @@ static dim3 panel_grid(int M, int jb, int k)
 // Rgetrf.cpp:95-132 with the device kernels above.  `ws` holds the pivot record, the
 // scratch column and the trailing GEMM's workspace.
 cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *ws,
-                          cudaStream_t st)
+                          cudaStream_t st, int max_ctas)
 {
     const int mn = imin(m, n);
     if (nb < 1)
@@ -1378,7 +1379,7 @@ cudaError_t rgetrf_launch(int m, int n, uint32_t *A, int lda, int *ipiv, int nb,
         const int M = m - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j; // indexed by panel-local row
-        const PanelForm pf = panel_form(M, jb);
+        const PanelForm pf = panel_form(M, jb, max_ctas);
         if (pf.ncta > 0) {
             cudaError_t e = launch_panel_cluster(lu_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, ipiv, info);
             if (e != cudaSuccess)
@@ -1431,7 +1432,8 @@ size_t rpotrf_workspace_bytes(int n, int nb)
 }
 
 // Lower Cholesky (Rpotrf.cpp:124-142 / Rpotrf2.cpp:132-146 order, blocked right-looking).
-cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st)
+cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, void *ws, cudaStream_t st,
+                                int max_ctas)
 {
     if (nb < 1)
         nb = 1;
@@ -1444,7 +1446,7 @@ cudaError_t rpotrf_lower_launch(int n, uint32_t *A, int lda, int nb, int *info, 
         const int M = n - j;
         uint32_t *P = A + j + (size_t)j * L;
         uint32_t *lc = lcol + j;
-        const PanelForm pf = panel_form(M, jb);
+        const PanelForm pf = panel_form(M, jb, max_ctas);
         if (pf.ncta > 0) {
             cudaError_t e = launch_panel_cluster(chol_panel_cluster_kernel, pf, jb, st, P, L, M, jb, pf.R, j, info);
             if (e != cudaSuccess)

@@ -160,6 +160,8 @@ namespace {
 // more requests per second (the serving burst: 656 solves/s at nb = 32 against 567 at the
 // tuned 16, 523 at 64, 457 at 128).  The bits do not depend on nb.
 constexpr int SERVE_MIN_NB = 32;
+// Largest thread-block cluster of a served unit's panels (0: the library's 8).
+constexpr int SERVE_PANEL_CTAS = 0;
 int serve_nb(const posit_server *s, int kind, int n)
 {
     return s->nb > 0 ? s->nb : std::max(SERVE_MIN_NB, pg::tuned_panel_width(kind == POSIT_BATCH_LU, n));
@@ -379,8 +381,10 @@ int launch_blocked(posit_server *s, Unit *u)
         void *ws = nullptr;
         SV_TRY(cudaMallocFromPoolAsync(&ws, ws_bytes(s, r.q.kind, n), s->pool, st));
         cudaError_t e = r.q.kind == POSIT_BATCH_LU
-                            ? pg::rgetrf_launch(n, n, f->dA, n, f->dipiv, serve_nb(s, r.q.kind, n), f->dinfo, ws, st)
-                            : pg::rpotrf_lower_launch(n, f->dA, n, serve_nb(s, r.q.kind, n), f->dinfo, ws, st);
+                            ? pg::rgetrf_launch(n, n, f->dA, n, f->dipiv, serve_nb(s, r.q.kind, n), f->dinfo, ws, st,
+                                                SERVE_PANEL_CTAS)
+                            : pg::rpotrf_lower_launch(n, f->dA, n, serve_nb(s, r.q.kind, n), f->dinfo, ws, st,
+                                                      SERVE_PANEL_CTAS);
         cudaFreeAsync(ws, st);
         if (e != cudaSuccess)
             return fail_code(e);
