@@ -99,6 +99,9 @@ size_t posit_rgemm_workspace_size(char transa, char transb, int m, int n, int k)
  * (Rgetrs.cpp:84-113), Rpotrf and Rpotrs with uplo 'L' or 'U' (Rpotrf.cpp:96-143,
  * Rpotrs.cpp:84-106). */
 #define POSIT_RPOTRF_UPPER_DEFAULT_NB 64
+/* The panel width nb <= 0 selects for an n x n LU (lu = 1) or lower Cholesky (lu = 0);
+ * host-only, no device needed. */
+int posit_tuned_panel_width(int lu, int n);
 
 /* Rgetrf (libRpack/Rgetrf.cpp:32-137; mplapack_posit.h:48), Rgetrf_opencl (mplapack_posit.h:49) */
 int posit_rgetrf_dev(int m, int n, uint32_t *A, int lda, int *ipiv, int nb, int *info, void *stream);

@@ -151,11 +151,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_TABLE)
     ap.add_argument("--per-bucket", type=int, default=150)
+    ap.add_argument("--sizes", default="256,512,1024,2048,4096,8192", help="panel widths: matrix sizes")
     args = ap.parse_args()
     import torch
     t0 = time.time()
     tiles, tdet = tune_gemm_tiles(args.per_bucket)
-    widths, wdet = tune_panel_width()
+    widths, wdet = tune_panel_width(sizes=tuple(int(x) for x in args.sizes.split(",")))
     res = {"device": torch.cuda.get_device_name(), "gemm_tile_table": tiles, "panel_width": widths,
            "detail": {"gemm_tiles": tdet, "panel_width": wdet}, "seconds": round(time.time() - t0, 1)}
     with open(args.out, "w") as f:

@@ -260,6 +260,8 @@ int posit_rgetrs_dev(char trans, int n, int nrhs, const uint32_t *A, int lda, co
     return 0;
 }
 
+int posit_tuned_panel_width(int lu, int n) { return pg::tuned_panel_width(lu != 0, n); }
+
 int posit_rpotrf_dev(char uplo, int n, uint32_t *A, int lda, int nb, int *info, void *stream)
 {
     bool upper = same(uplo, 'U');

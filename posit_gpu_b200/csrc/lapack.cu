@@ -1294,8 +1294,8 @@ int tuned_panel_width(bool lu, int n)
     struct Row {
         int n, lu, chol;
     };
-    static const Row rows[] = {{0, 16, 16}, {512, 16, 16}, {1024, 16, 16}, {2048, 16, 16}, {4096, 16, 16},
-                               {8192, 128, 24}};
+    static const Row rows[] = {{0, 24, 16},    {512, 24, 24},  {1024, 24, 16},   {2048, 24, 24},
+                               {4096, 32, 32}, {8192, 32, 24}, {16384, 128, 128}};
     int nb = 16;
     for (const Row &r : rows)
         if (n >= r.n)

@@ -101,3 +101,22 @@ def test_server_needs_a_device_and_reports_it():
                        (pg.E_NOT_CACHED, b"cached"), (pg.E_MISMATCH, b"matrix id"),
                        (pg.E_UNKNOWN_TICKET, b"ticket")):
         assert text in pg._lib.posit_strerror(code)
+
+
+def test_built_in_panel_widths_match_the_tuning_table():
+    """The widths nb <= 0 selects (compiled into the library) are the autotuner's table
+    committed beside it (posit_gpu_b200/tuning_b200.json), for every tuned size and the
+    sizes between."""
+    import json
+    import posit_gpu_b200 as pg
+    lib = ctypes.CDLL(pg.LIB_PATH)
+    lib.posit_tuned_panel_width.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.posit_tuned_panel_width.restype = ctypes.c_int
+    table = json.load(open(os.path.join(ROOT, "posit_gpu_b200", "tuning_b200.json")))["panel_width"]
+    for kind, lu in (("lu", 1), ("chol", 0)):
+        sizes = sorted(int(x) for x in table[kind])
+        for i, n in enumerate(sizes):
+            want = table[kind][str(n)]
+            upto = sizes[i + 1] - 1 if i + 1 < len(sizes) else 2 * n
+            for m in (n, (n + upto) // 2, upto):
+                assert lib.posit_tuned_panel_width(lu, m) == want, (kind, m)
