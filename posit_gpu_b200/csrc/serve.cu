@@ -157,8 +157,8 @@ namespace {
 // least SERVE_MIN_NB.  The tuned widths minimise one factorization's time alone; with many
 // units sharing the GPU the panels' latency hides behind other units and the trailing
 // GEMMs' efficiency counts (k = 16 runs at 64 % of k = 256's rate), so wider panels serve
-// more requests per second (the serving burst: 656 solves/s at nb = 32 against 567 at the
-// tuned 16, 523 at 64, 457 at 128).  The bits do not depend on nb.
+// more requests per second (the serving burst: 656 solves/s at nb = 32 against 567 at 16,
+// then the tuned width up to n = 4096, 523 at 64, 457 at 128).  The bits do not depend on nb.
 constexpr int SERVE_MIN_NB = 32;
 // Largest thread-block cluster of a served unit's panels (0: the library's 8).
 constexpr int SERVE_PANEL_CTAS = 0;
