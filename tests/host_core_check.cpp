@@ -322,6 +322,83 @@ long hc_split_round_check(uint64_t seed, long n)
     }
     return bad;
 }
+// The cluster LU panel (lapack.cu, lu_panel_cluster_kernel) restated on the host with the
+// same FP64 steps and rounding-constant table: rows stay in their slots, an interchange
+// swaps the logical row numbers two slots hold, the pivot is the largest key with the lowest
+// logical row among equal keys, and a zero pivot below row k trades back the two slots'
+// column-k values.  P is M x jb, column-major with ld M; ipiv receives 1-based pivots;
+// returns info (the first zero pivot, 1-based, or 0).
+int hc_lu_panel_relabel(uint32_t *P, int M, int jb, int *ipiv)
+{
+    std::vector<uint32_t> tab(F64_CONST_ENTRIES);
+    for (int i = 0; i < F64_CONST_ENTRIES; ++i)
+        tab[i] = f64_round_const_top((uint32_t)i);
+    const F64ConstTable cof{tab.data()};
+    std::vector<double> S((size_t)M * jb); // slot s, column c at S[s * jb + c]
+    std::vector<int> row(M);
+    for (int s = 0; s < M; ++s) {
+        row[s] = s;
+        for (int c = 0; c < jb; ++c)
+            S[(size_t)s * jb + c] = p32_to_double(P[s + (size_t)c * M]);
+    }
+    int info = 0;
+    std::vector<double> u(jb > 0 ? jb : 1);
+    for (int k = 0; k < jb; ++k) {
+        int ws = -1, br = -1;
+        double bk = -2.0, bv = 0.0;
+        for (int s = 0; s < M; ++s)
+            if (row[s] >= k) {
+                const double v = S[(size_t)s * jb + k], key = v != v ? -1.0 : (v < 0 ? -v : v);
+                if (br < 0 || key > bk || (key == bk && row[s] < br)) {
+                    bk = key;
+                    bv = v;
+                    br = row[s];
+                    ws = s;
+                }
+            }
+        const int p = br;
+        const uint32_t piv = p32_from_double_exact(bv);
+        for (int c = k + 1; c < jb; ++c)
+            u[c] = -S[(size_t)ws * jb + c];
+        int mode = 0;
+        uint32_t recip = 0;
+        if (piv == 0) {
+            if (info == 0)
+                info = k + 1;
+        } else if ((int32_t)pabs(piv) >= 1) {
+            mode = 1;
+            recip = pdiv_est(P32_ONE, piv);
+        } else {
+            mode = 2;
+        }
+        ipiv[k] = p + 1;
+        if (p != k) {
+            if (piv == 0)
+                for (int s = 0; s < M; ++s)
+                    if (row[s] == k) {
+                        S[(size_t)ws * jb + k] = S[(size_t)s * jb + k];
+                        S[(size_t)s * jb + k] = bv;
+                    }
+            for (int s = 0; s < M; ++s)
+                row[s] = row[s] == k ? p : (row[s] == p ? k : row[s]);
+        }
+        const double drecip = p32_to_double(recip);
+        for (int s = 0; s < M; ++s)
+            if (row[s] > k) {
+                double *rw = &S[(size_t)s * jb];
+                const double dl = mode == 1   ? f64_posit_mul_checked(rw[k], drecip, cof)
+                                  : mode == 2 ? p32_to_double(pdiv_est(p32_from_double_exact(rw[k]), piv))
+                                              : rw[k];
+                rw[k] = dl;
+                for (int c = k + 1; c < jb; ++c)
+                    rw[c] = f64_posit_mac_checked(rw[c], u[c], dl, cof);
+            }
+    }
+    for (int s = 0; s < M; ++s)
+        for (int c = 0; c < jb; ++c)
+            P[row[s] + (size_t)c * M] = p32_from_double_exact(S[(size_t)s * jb + c]);
+    return info;
+}
 // chain_add_run_reg against chain_add_run on one chain of n terms (patterns); 1 on a match
 int hc_chain_reg_check(uint32_t c0, const uint32_t *qp, int n)
 {

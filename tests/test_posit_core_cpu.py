@@ -409,6 +409,48 @@ def test_split_rounding_is_nearest_even_at_every_width(hc):
     assert hc.hc_split_round_check(20261204, 200_000) == 0
 
 
+def _panel_cases(rng):
+    for M, jb in ((1, 1), (5, 3), (40, 16), (300, 24), (130, 64)):
+        yield "random", M, jb, oracle.from_double(rng.uniform(-1, 1, M * jb))
+    for M, jb in ((64, 16), (200, 24)):  # few distinct magnitudes: equal keys, first row wins
+        yield "ties", M, jb, oracle.from_double(rng.choice([-1.0, 1.0, 0.5, -0.5, 2.0], M * jb))
+    A = oracle.from_double(rng.uniform(-1, 1, 100 * 16)).reshape(100, 16, order="F")
+    A[:, 5] = 0  # a zero column: zero pivot, no interchange needed
+    A[30, :] = 0
+    yield "zero column", 100, 16, np.ascontiguousarray(A.reshape(-1, order="F"))
+    for M in (80, 1000):  # NaR on the diagonal over zeros: a zero pivot below row 0
+        A = oracle.from_double(rng.uniform(-1, 1, M * 16)).reshape(M, 16, order="F")
+        A[:, 0] = 0
+        A[0, 0] = oracle.P32_NAR
+        yield "NaR over zeros", M, 16, np.ascontiguousarray(A.reshape(-1, order="F"))
+    A = oracle.from_double(rng.uniform(-1, 1, 90 * 8)).reshape(90, 8, order="F")
+    A[:, 3] = oracle.P32_NAR  # an all-NaR column: a NaR pivot (element-wise division)
+    yield "NaR column", 90, 8, np.ascontiguousarray(A.reshape(-1, order="F"))
+    A = oracle.from_double(rng.uniform(-1, 1, 120 * 12) * 1e-12).reshape(120, 12, order="F")
+    yield "tiny", 120, 12, np.ascontiguousarray(A.reshape(-1, order="F"))
+
+
+def test_cluster_lu_panel_restated_matches_the_reference_recursion(hc):
+    """The cluster LU panel's algorithm (rows kept in place, interchanges as relabelling,
+    the first-max pivot over logical rows, a zero pivot below the diagonal trading the two
+    rows' column back, the FP64 steps with the table of rounding constants) equals the
+    reference's recursive Rgetrf2 (the oracle) bit for bit, pivots and info included, on
+    random, tie-heavy, singular, NaR and tiny panels."""
+    hc.hc_lu_panel_relabel.restype = ctypes.c_int
+    hc.hc_lu_panel_relabel.argtypes = [np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS"),
+                                       ctypes.c_int, ctypes.c_int,
+                                       np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")]
+    rng = np.random.default_rng(77)
+    for name, M, jb, A in _panel_cases(rng):
+        g, o = A.copy(), A.copy()
+        pg_, po = np.zeros(jb, np.int32), np.zeros(jb, np.int32)
+        info_g = hc.hc_lu_panel_relabel(g, M, jb, pg_)
+        info_o = oracle.orc.orc_rgetrf2(M, jb, o, M, po)
+        assert info_g == info_o, name
+        assert np.array_equal(pg_, po), name
+        assert np.array_equal(g, o), name
+
+
 def test_exact_encode_round_trips_every_pattern_class(hc):
     """p32_from_double_exact (field assembly without rounding, for values that are posits)
     inverts p32_to_double on random patterns, every regime length and its neighbours,
