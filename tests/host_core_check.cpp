@@ -399,6 +399,48 @@ int hc_lu_panel_relabel(uint32_t *P, int M, int jb, int *ipiv)
             P[row[s] + (size_t)c * M] = p32_from_double_exact(S[(size_t)s * jb + c]);
     return info;
 }
+// The cluster Cholesky panel (lapack.cu, chol_panel_cluster_kernel) restated on the host
+// with the same FP64 steps: per column, l_kk = sqrt(a_kk) and 1/l_kk from the holder of row
+// k (a_kk <= 0 or NaR stops with info), the column below scaled by 1/l_kk (the FP64 product
+// step), then each row's entries up to the diagonal block's edge updated.  P is M x jb
+// (M >= jb), column-major with ld M; returns info.
+int hc_chol_panel(uint32_t *P, int M, int jb)
+{
+    std::vector<uint32_t> tab(F64_CONST_ENTRIES);
+    for (int i = 0; i < F64_CONST_ENTRIES; ++i)
+        tab[i] = f64_round_const_top((uint32_t)i);
+    const F64ConstTable cof{tab.data()};
+    std::vector<double> S((size_t)M * jb);
+    for (int i = 0; i < M; ++i)
+        for (int c = 0; c < jb; ++c)
+            S[(size_t)i * jb + c] = p32_to_double(P[i + (size_t)c * M]);
+    int info = 0;
+    std::vector<double> l(jb > 0 ? jb : 1);
+    for (int k = 0; k < jb; ++k) {
+        const uint32_t akk = p32_from_double_exact(S[(size_t)k * jb + k]);
+        if ((int32_t)akk <= 0) {
+            info = k + 1;
+            break;
+        }
+        const uint32_t lkk = psqrt_est(akk);
+        S[(size_t)k * jb + k] = p32_to_double(lkk);
+        const double drecip = p32_to_double(pdiv_est(P32_ONE, lkk));
+        for (int i = k + 1; i < M; ++i)
+            S[(size_t)i * jb + k] = f64_posit_mul_checked(S[(size_t)i * jb + k], drecip, cof);
+        for (int c = k + 1; c < jb; ++c)
+            l[c] = -S[(size_t)c * jb + k];
+        for (int i = k + 1; i < M; ++i) {
+            double *rw = &S[(size_t)i * jb];
+            const int cend = i < jb - 1 ? i : jb - 1;
+            for (int c = k + 1; c <= cend; ++c)
+                rw[c] = f64_posit_mac_checked(rw[c], l[c], rw[k], cof);
+        }
+    }
+    for (int i = 0; i < M; ++i)
+        for (int c = 0; c < jb; ++c)
+            P[i + (size_t)c * M] = p32_from_double_exact(S[(size_t)i * jb + c]);
+    return info;
+}
 // chain_add_run_reg against chain_add_run on one chain of n terms (patterns); 1 on a match
 int hc_chain_reg_check(uint32_t c0, const uint32_t *qp, int n)
 {

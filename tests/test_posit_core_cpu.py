@@ -451,6 +451,35 @@ def test_cluster_lu_panel_restated_matches_the_reference_recursion(hc):
         assert np.array_equal(g, o), name
 
 
+def test_cluster_cholesky_panel_restated_matches_the_reference(hc):
+    """The cluster Cholesky panel's algorithm (the holder of row k forms l_kk and 1/l_kk,
+    the column below scaled by the FP64 product step, the rows updated up to the diagonal
+    block's edge) equals the first jb columns of the reference's blocked Rpotrf('L') at
+    nb = jb (the oracle) bit for bit on SPD panels, and gives the same info where a leading
+    minor fails."""
+    hc.hc_chol_panel.restype = ctypes.c_int
+    hc.hc_chol_panel.argtypes = [np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS"),
+                                 ctypes.c_int, ctypes.c_int]
+    rng = np.random.default_rng(78)
+    for M, jb, bad in ((1, 1, -1), (16, 16, -1), (100, 16, -1), (300, 24, -1), (257, 64, -1),
+                       (200, 32, 20), (60, 16, 0)):
+        X = rng.uniform(-1, 1, (M, M))
+        S = oracle.from_double((X @ X.T / M + np.eye(M)).reshape(-1, order="F")).reshape(M, M, order="F")
+        if bad >= 0:
+            S[bad, bad] = oracle.p32(-1.0)
+        S = np.ascontiguousarray(S.reshape(-1, order="F"))
+        full = S.copy()
+        info_o = oracle.orc.orc_rpotrf(b"L", M, full, M, jb)
+        panel = np.ascontiguousarray(S.reshape(M, M, order="F")[:, :jb].reshape(-1, order="F"))
+        info_g = hc.hc_chol_panel(panel, M, jb)
+        if bad >= 0:
+            assert info_g == info_o == bad + 1, (M, jb)
+            continue
+        want = np.ascontiguousarray(full.reshape(M, M, order="F")[:, :jb].reshape(-1, order="F"))
+        assert info_g == info_o == 0
+        assert np.array_equal(panel, want), (M, jb)
+
+
 def test_exact_encode_round_trips_every_pattern_class(hc):
     """p32_from_double_exact (field assembly without rounding, for values that are posits)
     inverts p32_to_double on random patterns, every regime length and its neighbours,
